@@ -1,0 +1,123 @@
+"""ctypes bindings of libgdock.so (include/gdock.h).
+
+The library is the product: there is no Python or CPU fallback.  Loading
+fails with an error if libgdock.so is missing, and every call that returns a
+negative status raises GdockError with the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libgdock.so"
+
+GD_OK = 0
+GD_E_INVALID = -1
+GD_E_NOMEM = -2
+GD_E_CAPACITY = -3
+GD_E_CUDA = -4
+GD_E_TIMEOUT = -5
+GD_E_NODEVICE = -6
+GD_E_STATE = -7
+GD_E_BUSY = -8
+GD_E_CANCELLED = -9
+
+GD_KERNEL_BATCHED = 0
+GD_KERNEL_PLAIN = 1
+GD_PREC_FP32 = 0
+GD_PREC_FP32_KAHAN = 1
+GD_PREC_FP64 = 2
+
+# Every extern "C" symbol include/gdock.h declares.
+EXPORTED = [
+    "gd_last_error", "gd_set_ngpu", "gd_get_ngpu",
+    "SetDevice", "DeviceAlloc", "DeviceFree", "SetParaT", "CopyH2D", "InitCurand", "gd_rng_seed", "Dock",
+    "gd_set_option", "gd_get_option", "gd_eval_poses",
+    "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
+    "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
+    "gd_ensemble_autotune", "gd_ensemble_destroy",
+    "gd_layout", "gd_optimize_enepara",
+]
+
+
+class GdockError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gdock error {code}: {msg}")
+        self.code = code
+
+
+class JobDesc(C.Structure):
+    """gd_job_desc_t."""
+    _fields_ = [
+        ("natom", C.c_int), ("nlig", C.c_int),
+        ("lig_xyz", C.c_void_p), ("lig_type", C.c_void_p), ("lig_charge", C.c_void_p), ("lig_center", C.c_void_p),
+        ("pocket", C.c_int),
+        ("nkde", C.c_int), ("kde_xyz", C.c_void_p), ("kde_type", C.c_void_p),
+        ("nmcs", C.c_int), ("mcs_xyz", C.c_void_p), ("mcs_tcc", C.c_void_p),
+        ("psp_ncol", C.c_int), ("psp", C.c_void_p),
+        ("ntmp", C.c_int), ("temperature", C.c_void_p),
+        ("move_scale", C.c_float * 6),
+        ("seed", C.c_uint64),
+    ]
+
+
+class PocketDesc(C.Structure):
+    """gd_pocket_desc_t."""
+    _fields_ = [
+        ("npoint", C.c_int), ("nconf", C.c_int),
+        ("xyz", C.c_void_p), ("type", C.c_void_p), ("cls", C.c_void_p), ("cdc", C.c_void_p),
+        ("seq3r", C.c_void_p), ("hpp", C.c_void_p), ("ele", C.c_void_p), ("center", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load libgdock.so once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise GdockError(GD_E_STATE, f"{p} not built (python -m geauxdock_b200.build)")
+    lib = C.CDLL(str(p))
+    vp, ip, i, ll = C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_longlong
+    sig = {
+        "gd_last_error": (C.c_char_p, []),
+        "gd_set_ngpu": (i, [i]), "gd_get_ngpu": (i, []),
+        "SetDevice": (i, []), "DeviceAlloc": (i, [vp, vp, vp]), "DeviceFree": (i, [vp, vp, vp]),
+        "SetParaT": (i, [vp, vp]), "CopyH2D": (i, [vp, vp, vp]), "InitCurand": (i, [vp]),
+        "gd_rng_seed": (i, [vp, C.c_uint64]), "Dock": (i, [vp, vp, vp, vp, vp, vp]),
+        "gd_set_option": (i, [C.c_char_p, ll]), "gd_get_option": (ll, [C.c_char_p]),
+        "gd_eval_poses": (i, [vp, i, vp, vp, i, vp, vp, vp]),
+        "gd_ensemble_create": (i, [vp, i, vp, i, vp, i, vp]),
+        "gd_ensemble_create_complex": (i, [vp, i, vp, i, vp]),
+        "gd_ensemble_init": (i, [vp]), "gd_ensemble_run": (i, [vp, i, i]),
+        "gd_ensemble_sync": (i, [vp, C.POINTER(C.c_double), ip]),
+        "gd_ensemble_num_replicas": (i, [vp, i]), "gd_ensemble_replicas": (i, [vp, i, vp]),
+        "gd_ensemble_stats": (i, [vp, i, vp]), "gd_ensemble_autotune": (i, [vp, i, C.c_char_p, i]),
+        "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),
+        "gd_optimize_enepara": (i, [vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> int:
+    """Raise GdockError for a negative status."""
+    if rc < 0:
+        msg = load().gd_last_error()
+        raise GdockError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def layout(what: str) -> int:
+    return int(load().gd_layout(what.encode()))

@@ -1,0 +1,1052 @@
+// gd_api.cu -- the C ABI of libgdock.so: resident ensembles, the drop-in
+// Dock family, and pose evaluation.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "gd_pack.h"
+
+using namespace gd;
+
+namespace {
+
+struct Options {
+  int kernel = GD_KERNEL_BATCHED;
+  int precision = GD_PREC_FP32;
+  int warps = 0;  // 0: choose from occupancy
+  int kpl = 1;
+  int ab = 8;
+};
+Options g_opt;
+int g_ngpu = -1;
+std::mutex g_mu;
+
+int ngpu()
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_ngpu < 0) {
+    const char *e = std::getenv("GDOCK_NGPU");
+    g_ngpu = e ? std::max(1, std::atoi(e)) : 1;
+  }
+  return g_ngpu;
+}
+
+Options opts()
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_opt;
+}
+
+constexpr size_t kSmemLimit = 227 * 1024;
+constexpr int kExchTag = 1;
+
+}  // namespace
+
+struct gd_rng {
+  uint64_t seed = 0;
+  uint64_t calls = 0;
+  int seeded = 0;
+};
+
+struct gd_ensemble {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::vector<DevPocket> pockets;
+  std::vector<DevJobBuf> jobs;
+  std::vector<std::vector<int>> rep_prt;  // per job, per replica: protein conformation
+  DevJob *d_jobs = nullptr;
+  WorkItem *d_items = nullptr;
+  int n_items = 0;
+  int *d_queue = nullptr;
+  int *d_err = nullptr;
+  int kernel = GD_KERNEL_BATCHED;
+  int precision = GD_PREC_FP32;
+  TileConfig tc{8, 1, 8};
+  int grid = 0;
+  size_t smem = 0;
+  int Pmax = 0, Kmax = 0, Kst = 0, lig_slots = 0;
+  int step = 0;
+  // timing of the Monte Carlo launches
+  std::vector<cudaEvent_t> ev;
+  int ev_used = 0;
+  int launches = 0;
+};
+
+namespace {
+
+int set_device(int d) { GD_CUDA(cudaSetDevice(d)); return GD_OK; }
+
+// Work items: runs of consecutive replicas of one job with the same protein
+// conformation, at most `warps` long; heaviest (L x P) first.
+int build_items(gd_ensemble *e)
+{
+  std::vector<WorkItem> items;
+  std::vector<double> cost;
+  const int R = e->tc.warps_per_cta;
+  for (int j = 0; j < (int)e->jobs.size(); ++j) {
+    const std::vector<int> &pr = e->rep_prt[j];
+    const double c = (double)e->jobs[j].dj.natom * e->jobs[j].dj.npoint_pad;
+    int r = 0;
+    const int n = (int)pr.size();
+    while (r < n) {
+      int k = 1;
+      while (r + k < n && k < R && pr[r + k] == pr[r]) ++k;
+      items.push_back(WorkItem{j, pr[r], r, k});
+      cost.push_back(c);
+      r += k;
+    }
+  }
+  std::vector<int> ord(items.size());
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<WorkItem> sorted(items.size());
+  for (size_t i = 0; i < ord.size(); ++i) sorted[i] = items[ord[i]];
+  if (e->d_items) cudaFree(e->d_items);
+  e->d_items = nullptr;
+  e->n_items = (int)sorted.size();
+  if (!sorted.empty()) {
+    GD_CUDA(cudaMalloc(&e->d_items, sizeof(WorkItem) * sorted.size()));
+    GD_CUDA(cudaMemcpy(e->d_items, sorted.data(), sizeof(WorkItem) * sorted.size(), cudaMemcpyHostToDevice));
+  }
+  return GD_OK;
+}
+
+size_t smem_for(const gd_ensemble *e, int warps, int kst)
+{
+  return kernel_smem_bytes(e->Pmax, kst, e->lig_slots, warps, e->precision);
+}
+
+// Pick the KDE staging, the grid and (if not given) the replicas per CTA.
+int configure(gd_ensemble *e, TileConfig tc)
+{
+  if (tc.warps_per_cta < 1 || tc.warps_per_cta * 32 > kMaxCtaThreads)
+    return fail(GD_E_INVALID, "replicas per CTA = %d outside [1, %d]", tc.warps_per_cta, kMaxCtaThreads / 32);
+  e->Kst = e->Kmax;
+  if (smem_for(e, tc.warps_per_cta, e->Kst) > kSmemLimit) e->Kst = 0;  // KDE read from global memory
+  const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst);
+  if (smem > kSmemLimit)
+    return fail(GD_E_CAPACITY, "pocket of %d points needs %zu B of shared memory (limit %zu)", e->Pmax, smem, kSmemLimit);
+  const int occ = kernel_occupancy(0, e->precision, tc, smem);
+  if (occ < 1) return fail(GD_E_INVALID, "tile (warps %d, kpl %d, ab %d) cannot launch", tc.warps_per_cta, tc.kpl, tc.ab);
+  int nsm = 0;
+  GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+  e->tc = tc;
+  e->smem = smem;
+  GD_TRY(build_items(e));
+  e->grid = std::max(1, std::min(e->n_items, occ * nsm));
+  return GD_OK;
+}
+
+// Replicas per CTA from occupancy: fewest waves of work items, then most
+// resident warps per SM.
+int choose_warps(gd_ensemble *e, TileConfig base)
+{
+  int nsm = 0;
+  GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+  double best = 1e300;
+  int best_w = 8;
+  for (int w = 2; w <= kMaxCtaThreads / 32; ++w) {
+    TileConfig tc = base;
+    tc.warps_per_cta = w;
+    int kst = e->Kmax;
+    if (smem_for(e, w, kst) > kSmemLimit) kst = 0;
+    const size_t smem = smem_for(e, w, kst);
+    if (smem > kSmemLimit) continue;
+    const int occ = kernel_occupancy(0, e->precision, tc, smem);
+    if (occ < 1) continue;
+    // items and the slowest SM's load (items are equal-cost within a job)
+    long long items = 0;
+    for (size_t j = 0; j < e->jobs.size(); ++j) {
+      const std::vector<int> &pr = e->rep_prt[j];
+      int r = 0;
+      while (r < (int)pr.size()) {
+        int k = 1;
+        while (r + k < (int)pr.size() && k < w && pr[r + k] == pr[r]) ++k;
+        ++items;
+        r += k;
+      }
+    }
+    const long long slots = (long long)occ * nsm;
+    const long long waves = (items + slots - 1) / slots;
+    // time ~ waves * (warps resident per SM); fewer resident warps per SM than 16 also hurts latency hiding
+    const int resident = occ * w;
+    const double t = (double)waves * std::max(resident, 16) / (double)std::min(resident, 32);
+    if (t < best - 1e-9) {
+      best = t;
+      best_w = w;
+    }
+  }
+  TileConfig tc = base;
+  tc.warps_per_cta = best_w;
+  return configure(e, tc);
+}
+
+int upload_jobs(gd_ensemble *e)
+{
+  std::vector<DevJob> h(e->jobs.size());
+  for (size_t j = 0; j < e->jobs.size(); ++j) h[j] = e->jobs[j].dj;
+  if (e->d_jobs) cudaFree(e->d_jobs);
+  GD_CUDA(cudaMalloc(&e->d_jobs, sizeof(DevJob) * std::max<size_t>(h.size(), 1)));
+  GD_CUDA(cudaMemcpy(e->d_jobs, h.data(), sizeof(DevJob) * h.size(), cudaMemcpyHostToDevice));
+  return GD_OK;
+}
+
+int finish_create(gd_ensemble *e)
+{
+  e->Pmax = 0;
+  e->Kmax = 0;
+  int Lmax = 1;
+  e->rep_prt.resize(e->jobs.size());
+  for (size_t j = 0; j < e->jobs.size(); ++j) {
+    const DevJob &J = e->jobs[j].dj;
+    e->Pmax = std::max(e->Pmax, J.npoint_pad);
+    e->Kmax = std::max(e->Kmax, J.nkde);
+    Lmax = std::max(Lmax, J.natom);
+  }
+  e->lig_slots = (Lmax + 3) & ~3;
+  GD_TRY(upload_jobs(e));
+  GD_CUDA(cudaMalloc(&e->d_queue, sizeof(int)));
+  GD_CUDA(cudaMalloc(&e->d_err, sizeof(int)));
+  GD_CUDA(cudaMemset(e->d_err, 0, sizeof(int)));
+  GD_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+  const Options o = opts();
+  e->kernel = o.kernel;
+  e->precision = o.precision;
+  TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab};
+  if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
+  if (o.warps > 0) return configure(e, tc);
+  return choose_warps(e, tc);
+}
+
+int read_replica_prt(gd_ensemble *e, size_t j, const std::vector<ReplicaMC> &reps)
+{
+  e->rep_prt[j].resize(reps.size());
+  for (size_t r = 0; r < reps.size(); ++r) e->rep_prt[j][r] = reps[r].idx_prt;
+  return GD_OK;
+}
+
+cudaEvent_t next_event(gd_ensemble *e)
+{
+  if (e->ev_used == (int)e->ev.size()) {
+    cudaEvent_t x;
+    if (cudaEventCreate(&x) != cudaSuccess) return nullptr;
+    e->ev.push_back(x);
+  }
+  return e->ev[e->ev_used++];
+}
+
+int check_err(gd_ensemble *e)
+{
+  int h = 0;
+  GD_CUDA(cudaMemcpy(&h, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h & kErrTimeout) return fail(GD_E_TIMEOUT, "a bounded wait for a shared-memory bulk copy gave up");
+  return GD_OK;
+}
+
+int launch_mc(gd_ensemble *e, int s_begin, int nsteps, int flags)
+{
+  cudaEvent_t e0 = next_event(e), e1 = next_event(e);
+  if (!e0 || !e1) return fail(GD_E_CUDA, "cudaEventCreate failed");
+  GD_CUDA(cudaEventRecord(e0, e->st));
+  if (e->kernel == GD_KERNEL_PLAIN) {
+    for (size_t j = 0; j < e->jobs.size(); ++j)
+      GD_CUDA(launch_plain(e->d_jobs + j, e->jobs[j].dj.nrep, s_begin, nsteps, flags, e->d_err, e->st));
+    e->launches += (int)e->jobs.size();
+  } else {
+    GD_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
+    KArgs a{};
+    a.jobs = e->d_jobs;
+    a.items = e->d_items;
+    a.n_items = e->n_items;
+    a.queue = e->d_queue;
+    a.err = e->d_err;
+    a.s_begin = s_begin;
+    a.nsteps = nsteps;
+    a.flags = flags;
+    a.P = e->Pmax;
+    a.Kst = e->Kst;
+    a.lig_slots = e->lig_slots;
+    GD_CUDA(launch_kernel(0, e->precision, e->tc, a, e->grid, e->st));
+    e->launches += 1;
+  }
+  GD_CUDA(cudaEventRecord(e1, e->st));
+  return GD_OK;
+}
+
+int launch_exchange_all(gd_ensemble *e, int x)
+{
+  for (size_t j = 0; j < e->jobs.size(); ++j) {
+    const DevJob &J = e->jobs[j].dj;
+    if (J.ntmp < 2) continue;
+    GD_CUDA(launch_exchange(e->d_jobs + j, J.nprt * J.nlig, J.ntmp, x, e->st));
+  }
+  return GD_OK;
+}
+
+// nsteps steps from e->step, cut at exchange boundaries.
+int advance(gd_ensemble *e, int nsteps, int spx, int f_first, int f_all, int f_last)
+{
+  int done = 0;
+  while (done < nsteps) {
+    int chunk = nsteps - done;
+    if (spx > 0) chunk = std::min(chunk, spx - (e->step % spx));
+    const int f = f_all | (done == 0 ? f_first : 0) | (done + chunk == nsteps ? f_last : 0);
+    GD_TRY(launch_mc(e, e->step, chunk, f));
+    e->step += chunk;
+    done += chunk;
+    if (spx > 0 && e->step % spx == 0) GD_TRY(launch_exchange_all(e, e->step / spx - 1));
+  }
+  return GD_OK;
+}
+
+void destroy(gd_ensemble *e)
+{
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->st) cudaStreamSynchronize(e->st);
+  for (auto &j : e->jobs) free_job(j);
+  for (auto &p : e->pockets) free_pocket(p);
+  if (e->d_jobs) cudaFree(e->d_jobs);
+  if (e->d_items) cudaFree(e->d_items);
+  if (e->d_queue) cudaFree(e->d_queue);
+  if (e->d_err) cudaFree(e->d_err);
+  for (auto x : e->ev) cudaEventDestroy(x);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+}
+
+// Ensemble of one job from a Complex replica range (the Dock path).
+int ensemble_from_complex_range(const Complex *c, int rb, int re, uint64_t seed, Record *rec, int device,
+                                gd_ensemble **out)
+{
+  *out = nullptr;
+  GD_TRY(set_device(device));
+  PocketData pk;
+  JobData jd;
+  GD_TRY(pocket_from_complex(c, pk));
+  GD_TRY(job_from_complex(c, rb, re, seed, jd));
+  gd_ensemble *e = new gd_ensemble;
+  e->device = device;
+  e->pockets.resize(1);
+  e->jobs.resize(1);
+  int rc = pack_pocket(pk, e->pockets[0]);
+  if (rc == GD_OK) rc = pack_job(jd, e->pockets[0], c->enepara, rec != nullptr, rec, e->jobs[0]);
+  if (rc == GD_OK) {
+    e->rep_prt.resize(1);
+    read_replica_prt(e, 0, jd.reps);
+    rc = finish_create(e);
+  }
+  if (rc != GD_OK) {
+    destroy(e);
+    return rc;
+  }
+  *out = e;
+  return GD_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+int gd_set_ngpu(int n)
+{
+  if (n < 1) return fail(GD_E_INVALID, "ngpu = %d", n);
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_ngpu = n;
+  return GD_OK;
+}
+
+int gd_get_ngpu(void) { return ngpu(); }
+
+int gd_set_option(const char *name, long long v)
+{
+  if (!name) return fail(GD_E_INVALID, "null option name");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const std::string n(name);
+  if (n == "kernel") {
+    if (v != GD_KERNEL_BATCHED && v != GD_KERNEL_PLAIN) return fail(GD_E_INVALID, "kernel = %lld", v);
+    g_opt.kernel = (int)v;
+  } else if (n == "precision") {
+    if (v < GD_PREC_FP32 || v > GD_PREC_FP64) return fail(GD_E_INVALID, "precision = %lld", v);
+    g_opt.precision = (int)v;
+  } else if (n == "warps") {
+    if (v < 0 || v > kMaxCtaThreads / 32) return fail(GD_E_INVALID, "warps = %lld", v);
+    g_opt.warps = (int)v;
+  } else if (n == "kpl") {
+    if (v != 1 && v != 2 && v != 4) return fail(GD_E_INVALID, "kpl = %lld", v);
+    g_opt.kpl = (int)v;
+  } else if (n == "ab") {
+    if (v != 4 && v != 8) return fail(GD_E_INVALID, "ab = %lld", v);
+    g_opt.ab = (int)v;
+  } else {
+    return fail(GD_E_INVALID, "unknown option '%s'", name);
+  }
+  return GD_OK;
+}
+
+long long gd_get_option(const char *name)
+{
+  if (!name) return GD_E_INVALID;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const std::string n(name);
+  if (n == "kernel") return g_opt.kernel;
+  if (n == "precision") return g_opt.precision;
+  if (n == "warps") return g_opt.warps;
+  if (n == "kpl") return g_opt.kpl;
+  if (n == "ab") return g_opt.ab;
+  return GD_E_INVALID;
+}
+
+// ---------------------------------------------------------------- Dock --
+int SetDevice(void)
+{
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) return fail(GD_E_NODEVICE, "no CUDA device");
+  const int n = ngpu();
+  if (n > count) return fail(GD_E_NODEVICE, "%d GPUs requested, %d present", n, count);
+  for (int g = 0; g < n; ++g) {
+    GD_CUDA(cudaSetDevice(g));
+    GD_CUDA(cudaDeviceSetCacheConfig(cudaFuncCachePreferShared));  // prepair.C:11-20
+  }
+  return GD_OK;
+}
+
+int DeviceAlloc(Complex **cd, Record **rd, gd_rng_t **rng)
+{
+  if (!cd || !rd || !rng) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  for (int g = 0; g < n; ++g) {
+    GD_CUDA(cudaSetDevice(g));
+    cd[g] = nullptr;
+    rd[g] = nullptr;
+    if (cudaMalloc((void **)&cd[g], sizeof(Complex)) != cudaSuccess)
+      return fail(GD_E_NOMEM, "device Complex (%zu B) on GPU %d", sizeof(Complex), g);
+    if (cudaMalloc((void **)&rd[g], sizeof(Record) * (size_t)GD_MAX_REP) != cudaSuccess)
+      return fail(GD_E_NOMEM, "device Record[%d] on GPU %d", GD_MAX_REP, g);
+    rng[g] = new gd_rng;
+  }
+  return GD_OK;
+}
+
+int DeviceFree(Complex **cd, Record **rd, gd_rng_t **rng)
+{
+  if (!cd || !rd || !rng) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  for (int g = 0; g < n; ++g) {
+    GD_CUDA(cudaSetDevice(g));
+    if (cd[g]) GD_CUDA(cudaFree(cd[g]));
+    if (rd[g]) GD_CUDA(cudaFree(rd[g]));
+    delete rng[g];
+    cd[g] = nullptr;
+    rd[g] = nullptr;
+    rng[g] = nullptr;
+  }
+  return GD_OK;
+}
+
+int SetParaT(Complex *ch, ParaT **pt)
+{
+  if (!ch || !pt) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  const int n_rep = ch->size.n_rep;
+  if (n_rep < 1 || n_rep > GD_MAX_REP) return fail(GD_E_INVALID, "n_rep = %d", n_rep);
+  int per = (n_rep + n - 1) / n;  // prepair.C:366-375, maximising balance
+  const McPara &mp = ch->mcpara;
+  const bool exch = mp.steps_per_exchange > 0 && ch->size.n_tmp > 1;
+  if (exch && n > 1) {
+    // exchange partners share (protein conf, ligand conf): cut at protein-conformation blocks
+    const int block = ch->size.n_tmp * ch->size.n_lig;
+    per = ((ch->size.n_prt + n - 1) / n) * block;
+  }
+  const int n_active = (n_rep + per - 1) / per;
+  if (n_active < n) return fail(GD_E_INVALID, "%d replicas cannot keep %d GPUs busy", n_rep, n);
+  for (int g = 0; g < n; ++g) {
+    pt[g]->rep_begin = per * g;
+    pt[g]->rep_end = std::min(pt[g]->rep_begin + per, n_rep) - 1;
+    pt[g]->n_rep = pt[g]->rep_end - pt[g]->rep_begin + 1;
+    pt[g]->record_sz = (int)sizeof(Record) * pt[g]->n_rep;
+  }
+  return GD_OK;
+}
+
+int CopyH2D(Complex *ch, Complex **cd, ParaT **pt)
+{
+  if (!ch || !cd || !pt) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  for (int g = 0; g < n; ++g) {
+    GD_CUDA(cudaSetDevice(g));
+    ch->rep_begin = pt[g]->rep_begin;  // prepair.C:119-123
+    ch->rep_end = pt[g]->rep_end;
+    GD_CUDA(cudaMemcpy(cd[g], ch, sizeof(Complex), cudaMemcpyHostToDevice));
+  }
+  return GD_OK;
+}
+
+int InitCurand(gd_rng_t **rng)
+{
+  if (!rng) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  const char *env = std::getenv("GDOCK_SEED");
+  const uint64_t base = env ? std::strtoull(env, nullptr, 10) : (uint64_t)std::time(nullptr);
+  for (int g = 0; g < n; ++g) {
+    if (!rng[g]) return fail(GD_E_STATE, "InitCurand before DeviceAlloc");
+    if (!rng[g]->seeded) {
+      rng[g]->seed = base + (uint64_t)g;  // backend_gpu.cu:52-56: one seed per GPU
+      rng[g]->seeded = 1;
+    }
+    rng[g]->calls = 0;
+  }
+  return GD_OK;
+}
+
+int gd_rng_seed(gd_rng_t *rng, uint64_t seed)
+{
+  if (!rng) return fail(GD_E_INVALID, "null rng");
+  rng->seed = seed;
+  rng->seeded = 1;
+  rng->calls = 0;
+  return GD_OK;
+}
+
+int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_t **rng)
+{
+  if (!ch || !rh || !cd || !rd || !pt || !rng) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  const McPara &mp = ch->mcpara;
+  const int steps_total = mp.steps_total, spd = mp.steps_per_dump;
+  if (steps_total < 0) return fail(GD_E_INVALID, "steps_total = %d", steps_total);
+  if (spd < 1 || spd > GD_STEPS_PER_DUMP)
+    return fail(GD_E_INVALID, "steps_per_dump = %d outside [1, %d] (Record capacity)", spd, GD_STEPS_PER_DUMP);
+  const int spx = (mp.steps_per_exchange > 0 && ch->size.n_tmp > 1) ? mp.steps_per_exchange : 0;
+  std::vector<gd_ensemble *> ens(n, nullptr);
+  int rc = GD_OK;
+  for (int g = 0; g < n && rc == GD_OK; ++g) {
+    if (!rng[g] || !cd[g] || !rd[g]) {
+      rc = fail(GD_E_STATE, "Dock before DeviceAlloc/InitCurand on GPU %d", g);
+      break;
+    }
+    // each Dock call draws a fresh stream from the handle (the reference's curand state advances)
+    const uint64_t seed = rng[g]->seed + (rng[g]->calls++ << 32);
+    rc = ensemble_from_complex_range(ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], g, &ens[g]);
+  }
+  // initial energy, backend_gpu.cu:87-91: one step, no move, forced accept
+  for (int g = 0; g < n && rc == GD_OK; ++g) {
+    rc = set_device(g);
+    if (rc == GD_OK) rc = launch_mc(ens[g], 0, 1, kMcInitial | kMcRecord | kMcResetRecord | kMcStoreAccept);
+  }
+  // dump chunks, backend_gpu.cu:96-114
+  for (int s1 = 0; s1 < steps_total && rc == GD_OK; s1 += spd) {
+    for (int g = 0; g < n && rc == GD_OK; ++g) {
+      rc = set_device(g);
+      ens[g]->step = s1;
+      if (rc == GD_OK) rc = advance(ens[g], spd, spx, kMcResetRecord, kMcRecord, kMcStoreAccept);
+    }
+    for (int g = 0; g < n && rc == GD_OK; ++g) {
+      rc = set_device(g);
+      if (rc != GD_OK) break;
+      const cudaError_t ce = cudaMemcpyAsync(rh + pt[g]->rep_begin, rd[g], sizeof(Record) * (size_t)pt[g]->n_rep,
+                                             cudaMemcpyDeviceToHost, ens[g]->st);
+      if (ce == cudaSuccess) {
+        const cudaError_t se = cudaStreamSynchronize(ens[g]->st);
+        if (se != cudaSuccess) rc = fail(GD_E_CUDA, "Dock: %s", cudaGetErrorString(se));
+      } else {
+        rc = fail(GD_E_CUDA, "Dock record copy: %s", cudaGetErrorString(ce));
+      }
+      if (rc == GD_OK) rc = check_err(ens[g]);
+    }
+  }
+  // final replica states: device Complex (as the reference) and the host Complex
+  for (int g = 0; g < n && rc == GD_OK; ++g) {
+    rc = set_device(g);
+    if (rc != GD_OK) break;
+    const DevJob &J = ens[g]->jobs[0].dj;
+    const size_t bytes = sizeof(ReplicaMC) * (size_t)J.nrep;
+    if (cudaMemcpyAsync(cd[g]->replica + pt[g]->rep_begin, J.rep, bytes, cudaMemcpyDeviceToDevice, ens[g]->st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(ch->replica + pt[g]->rep_begin, J.rep, bytes, cudaMemcpyDeviceToHost, ens[g]->st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ens[g]->st) != cudaSuccess)
+      rc = fail(GD_E_CUDA, "Dock final copy on GPU %d", g);
+  }
+  for (int g = 0; g < n; ++g) destroy(ens[g]);
+  return rc;
+}
+
+// ------------------------------------------------------------ poses --
+int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int precision, float *out,
+                  double *out64, float *raw)
+{
+  if (!c || n < 0 || (n > 0 && (!conf || !mm || !out))) return fail(GD_E_INVALID, "null argument");
+  if (precision < GD_PREC_FP32 || precision > GD_PREC_FP64) return fail(GD_E_INVALID, "precision = %d", precision);
+  if (n == 0) return GD_OK;
+  for (int i = 0; i < n; ++i)
+    if (conf[2 * i] < 0 || conf[2 * i] >= c->size.n_lig || conf[2 * i + 1] < 0 || conf[2 * i + 1] >= c->size.n_prt)
+      return fail(GD_E_INVALID, "pose %d: conformation (%d, %d) out of range", i, conf[2 * i], conf[2 * i + 1]);
+  int dev = 0;
+  GD_CUDA(cudaGetDevice(&dev));
+  PocketData pk;
+  JobData jd;
+  GD_TRY(pocket_from_complex(c, pk));
+  GD_TRY(job_from_complex(c, 0, 0, 0, jd));
+  gd_ensemble *e = new gd_ensemble;
+  e->device = dev;
+  e->pockets.resize(1);
+  e->jobs.resize(1);
+  int rc = pack_pocket(pk, e->pockets[0]);
+  if (rc == GD_OK) rc = pack_job(jd, e->pockets[0], c->enepara, false, nullptr, e->jobs[0]);
+  if (rc != GD_OK) {
+    destroy(e);
+    return rc;
+  }
+  const Options o = opts();
+  e->precision = precision;
+  const DevJob &J = e->jobs[0].dj;
+  e->Pmax = J.npoint_pad;
+  e->Kmax = J.nkde;
+  e->lig_slots = (J.natom + 3) & ~3;
+  TileConfig tc{8, o.kpl, o.ab};
+  if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
+  e->Kst = e->Kmax;
+  if (smem_for(e, tc.warps_per_cta, e->Kst) > kSmemLimit) e->Kst = 0;
+  e->smem = smem_for(e, tc.warps_per_cta, e->Kst);
+  if (e->smem > kSmemLimit) {
+    destroy(e);
+    return fail(GD_E_CAPACITY, "pocket too large for shared memory");
+  }
+  // poses grouped by protein conformation so that a CTA stages one conformation
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return conf[2 * a + 1] < conf[2 * b + 1]; });
+  std::vector<int> sconf(2 * (size_t)n);
+  std::vector<float> smm(6 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    sconf[2 * i] = conf[2 * ord[i]];
+    sconf[2 * i + 1] = conf[2 * ord[i] + 1];
+    for (int k = 0; k < 6; ++k) smm[6 * i + k] = mm[6 * ord[i] + k];
+  }
+  std::vector<WorkItem> items;
+  for (int i = 0; i < n;) {
+    int k = 1;
+    while (i + k < n && k < tc.warps_per_cta && sconf[2 * (i + k) + 1] == sconf[2 * i + 1]) ++k;
+    items.push_back(WorkItem{0, sconf[2 * i + 1], i, k});
+    i += k;
+  }
+  int *d_conf = nullptr;
+  float *d_mm = nullptr, *d_out = nullptr, *d_raw = nullptr;
+  double *d_out64 = nullptr;
+  WorkItem *d_items = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(d_conf);
+    cudaFree(d_mm);
+    cudaFree(d_out);
+    cudaFree(d_raw);
+    cudaFree(d_out64);
+    cudaFree(d_items);
+    destroy(e);
+  };
+#define EV_CUDA(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t ce_ = (call);                                                                 \
+    if (ce_ != cudaSuccess) {                                                                 \
+      cleanup();                                                                              \
+      return fail(GD_E_CUDA, "gd_eval_poses: %s: %s", #call, cudaGetErrorString(ce_));        \
+    }                                                                                         \
+  } while (0)
+  EV_CUDA(upload_jobs(e) == GD_OK ? cudaSuccess : cudaErrorUnknown);
+  EV_CUDA(cudaMalloc(&e->d_queue, sizeof(int)));
+  EV_CUDA(cudaMalloc(&e->d_err, sizeof(int)));
+  EV_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+  EV_CUDA(cudaMalloc(&d_conf, sizeof(int) * 2 * n));
+  EV_CUDA(cudaMalloc(&d_mm, sizeof(float) * 6 * n));
+  EV_CUDA(cudaMalloc(&d_out, sizeof(float) * 10 * n));
+  if (raw) EV_CUDA(cudaMalloc(&d_raw, sizeof(float) * 9 * n));
+  if (out64) EV_CUDA(cudaMalloc(&d_out64, sizeof(double) * 10 * n));
+  EV_CUDA(cudaMalloc(&d_items, sizeof(WorkItem) * items.size()));
+  EV_CUDA(cudaMemcpyAsync(d_conf, sconf.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemcpyAsync(d_mm, smm.data(), sizeof(float) * 6 * n, cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
+  EV_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), e->st));
+  KArgs a{};
+  a.jobs = e->d_jobs;
+  a.items = d_items;
+  a.n_items = (int)items.size();
+  a.queue = e->d_queue;
+  a.err = e->d_err;
+  a.P = e->Pmax;
+  a.Kst = e->Kst;
+  a.lig_slots = e->lig_slots;
+  a.conf = d_conf;
+  a.mm = d_mm;
+  a.out = d_out;
+  a.out64 = d_out64;
+  a.raw = d_raw;
+  int nsm = 0;
+  EV_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int occ = std::max(1, kernel_occupancy(1, precision, tc, e->smem));
+  const int grid = std::max(1, std::min((int)items.size(), occ * nsm));
+  EV_CUDA(launch_kernel(1, precision, tc, a, grid, e->st));
+  std::vector<float> hout(10 * (size_t)n), hraw(raw ? 9 * (size_t)n : 0);
+  std::vector<double> hout64(out64 ? 10 * (size_t)n : 0);
+  EV_CUDA(cudaMemcpyAsync(hout.data(), d_out, sizeof(float) * 10 * n, cudaMemcpyDeviceToHost, e->st));
+  if (raw) EV_CUDA(cudaMemcpyAsync(hraw.data(), d_raw, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, e->st));
+  if (out64) EV_CUDA(cudaMemcpyAsync(hout64.data(), d_out64, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, e->st));
+  EV_CUDA(cudaStreamSynchronize(e->st));
+  int herr = 0;
+  EV_CUDA(cudaMemcpy(&herr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+#undef EV_CUDA
+  for (int i = 0; i < n; ++i) {
+    const int o = ord[i];
+    std::memcpy(out + 10 * (size_t)o, &hout[10 * (size_t)i], sizeof(float) * 10);
+    if (raw) std::memcpy(raw + 9 * (size_t)o, &hraw[9 * (size_t)i], sizeof(float) * 9);
+    if (out64) std::memcpy(out64 + 10 * (size_t)o, &hout64[10 * (size_t)i], sizeof(double) * 10);
+  }
+  cleanup();
+  if (herr) return fail(GD_E_TIMEOUT, "gd_eval_poses: bounded wait gave up");
+  return GD_OK;
+}
+
+// ---------------------------------------------------------- ensembles --
+int gd_ensemble_create(const gd_pocket_desc_t *pockets, int npocket, const gd_job_desc_t *jobs, int njob,
+                       const EnePara *enepara, int device, gd_ensemble_t **out)
+{
+  if (!out) return fail(GD_E_INVALID, "null out");
+  *out = nullptr;
+  if (!pockets || npocket < 1 || !jobs || njob < 1 || !enepara) return fail(GD_E_INVALID, "empty ensemble");
+  GD_TRY(set_device(device));
+  gd_ensemble *e = new gd_ensemble;
+  e->device = device;
+  e->pockets.resize(npocket);
+  e->jobs.resize(njob);
+  e->rep_prt.resize(njob);
+  int rc = GD_OK;
+  std::vector<int> nconf(npocket);
+  for (int p = 0; p < npocket && rc == GD_OK; ++p) {
+    PocketData pk;
+    rc = pocket_from_desc(pockets[p], pk);
+    if (rc == GD_OK) rc = pack_pocket(pk, e->pockets[p]);
+    nconf[p] = pockets[p].nconf;
+  }
+  for (int j = 0; j < njob && rc == GD_OK; ++j) {
+    const int p = jobs[j].pocket;
+    if (p < 0 || p >= npocket) {
+      rc = fail(GD_E_INVALID, "job %d: pocket %d out of range", j, p);
+      break;
+    }
+    JobData jd;
+    rc = job_from_desc(jobs[j], nconf[p], jd);
+    if (rc == GD_OK) rc = pack_job(jd, e->pockets[p], *enepara, false, nullptr, e->jobs[j]);
+    if (rc == GD_OK) read_replica_prt(e, j, jd.reps);
+    e->jobs[j].pocket = p;
+  }
+  if (rc == GD_OK) rc = finish_create(e);
+  if (rc != GD_OK) {
+    destroy(e);
+    return rc;
+  }
+  *out = e;
+  return GD_OK;
+}
+
+int gd_ensemble_create_complex(const Complex *const *cx, int n, const uint64_t *seeds, int device,
+                               gd_ensemble_t **out)
+{
+  if (!out) return fail(GD_E_INVALID, "null out");
+  *out = nullptr;
+  if (!cx || n < 1) return fail(GD_E_INVALID, "empty ensemble");
+  GD_TRY(set_device(device));
+  gd_ensemble *e = new gd_ensemble;
+  e->device = device;
+  e->jobs.resize(n);
+  e->rep_prt.resize(n);
+  std::vector<PocketData> seen;
+  int rc = GD_OK;
+  for (int j = 0; j < n && rc == GD_OK; ++j) {
+    PocketData pk;
+    JobData jd;
+    rc = pocket_from_complex(cx[j], pk);
+    if (rc == GD_OK) rc = job_from_complex(cx[j], 0, cx[j]->size.n_rep - 1, seeds ? seeds[j] : 0, jd);
+    if (rc != GD_OK) break;
+    // identical protein conformation sets share one device pocket
+    int p = -1;
+    for (size_t q = 0; q < seen.size(); ++q)
+      if (seen[q].nconf == pk.nconf && seen[q].npts == pk.npts && seen[q].xyz == pk.xyz && seen[q].type == pk.type &&
+          seen[q].cls == pk.cls && seen[q].cdc == pk.cdc && seen[q].seq3r == pk.seq3r && seen[q].hpp == pk.hpp &&
+          seen[q].ele == pk.ele && seen[q].center == pk.center) {
+        p = (int)q;
+        break;
+      }
+    if (p < 0) {
+      e->pockets.emplace_back();
+      rc = pack_pocket(pk, e->pockets.back());
+      seen.push_back(std::move(pk));
+      p = (int)seen.size() - 1;
+    }
+    if (rc == GD_OK) rc = pack_job(jd, e->pockets[p], cx[j]->enepara, false, nullptr, e->jobs[j]);
+    if (rc == GD_OK) read_replica_prt(e, j, jd.reps);
+    e->jobs[j].pocket = p;
+  }
+  if (rc == GD_OK) rc = finish_create(e);
+  if (rc != GD_OK) {
+    destroy(e);
+    return rc;
+  }
+  *out = e;
+  return GD_OK;
+}
+
+int gd_ensemble_init(gd_ensemble_t *e)
+{
+  if (!e) return fail(GD_E_INVALID, "null ensemble");
+  GD_TRY(set_device(e->device));
+  return launch_mc(e, 0, 1, kMcInitial | kMcStoreAccept);
+}
+
+int gd_ensemble_run(gd_ensemble_t *e, int nsteps, int steps_per_exchange)
+{
+  if (!e) return fail(GD_E_INVALID, "null ensemble");
+  if (nsteps < 0 || steps_per_exchange < 0) return fail(GD_E_INVALID, "nsteps = %d, steps_per_exchange = %d", nsteps, steps_per_exchange);
+  GD_TRY(set_device(e->device));
+  return advance(e, nsteps, steps_per_exchange, 0, 0, kMcStoreAccept);
+}
+
+int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches)
+{
+  if (!e) return fail(GD_E_INVALID, "null ensemble");
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  double ms = 0;
+  for (int i = 0; i + 1 < e->ev_used; i += 2) {
+    float t = 0;
+    GD_CUDA(cudaEventElapsedTime(&t, e->ev[i], e->ev[i + 1]));
+    ms += t;
+  }
+  if (kernel_ms) *kernel_ms = ms;
+  if (launches) *launches = e->launches;
+  e->ev_used = 0;
+  e->launches = 0;
+  return check_err(e);
+}
+
+int gd_ensemble_num_replicas(const gd_ensemble_t *e, int job)
+{
+  if (!e || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  return e->jobs[job].dj.nrep;
+}
+
+int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out)
+{
+  if (!e || !out || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  GD_TRY(set_device(e->device));
+  const DevJob &J = e->jobs[job].dj;
+  GD_CUDA(cudaMemcpyAsync(out, J.rep, sizeof(ReplicaMC) * (size_t)J.nrep, cudaMemcpyDeviceToHost, e->st));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  return GD_OK;
+}
+
+int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8)
+{
+  if (!e || !out8 || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  GD_TRY(set_device(e->device));
+  const DevJob &J = e->jobs[job].dj;
+  std::vector<RepStats> s(J.nrep);
+  GD_CUDA(cudaMemcpyAsync(s.data(), J.stats, sizeof(RepStats) * s.size(), cudaMemcpyDeviceToHost, e->st));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  for (int r = 0; r < J.nrep; ++r) {
+    const RepStats &x = s[r];
+    double *o = out8 + 8 * (size_t)r;
+    const double n = (double)x.n_steps;
+    o[0] = n;
+    o[1] = (double)x.n_accept;
+    o[2] = (double)x.n_exch_try;
+    o[3] = (double)x.n_exch_acc;
+    o[4] = n > 0 ? x.e_sum / n : 0.0;
+    o[5] = n > 0 ? std::max(0.0, x.e_sum2 / n - o[4] * o[4]) : 0.0;
+    o[6] = x.best_e;
+    o[7] = (double)x.best_step;
+  }
+  return GD_OK;
+}
+
+int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len)
+{
+  if (!e || steps < 1) return fail(GD_E_INVALID, "autotune: steps = %d", steps);
+  if (e->kernel != GD_KERNEL_BATCHED) return GD_OK;
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  // snapshot of everything a Monte Carlo launch writes (records are not written: no record flags)
+  std::vector<void *> snaps;
+  auto snap_bytes = [](const DevJob &J) {
+    return sizeof(ReplicaMC) * (size_t)J.nrep + sizeof(int) * (size_t)J.nrep + sizeof(RepStats) * (size_t)J.nrep;
+  };
+  int rc = GD_OK;
+  for (auto &jb : e->jobs) {
+    void *p = nullptr;
+    const DevJob &J = jb.dj;
+    if (cudaMalloc(&p, snap_bytes(J)) != cudaSuccess) {
+      rc = fail(GD_E_NOMEM, "autotune snapshot");
+      break;
+    }
+    unsigned char *b = (unsigned char *)p;
+    cudaMemcpyAsync(b, J.rep, sizeof(ReplicaMC) * J.nrep, cudaMemcpyDeviceToDevice, e->st);
+    cudaMemcpyAsync(b + sizeof(ReplicaMC) * J.nrep, J.run_acc, sizeof(int) * J.nrep, cudaMemcpyDeviceToDevice, e->st);
+    cudaMemcpyAsync(b + (sizeof(ReplicaMC) + sizeof(int)) * J.nrep, J.stats, sizeof(RepStats) * J.nrep,
+                    cudaMemcpyDeviceToDevice, e->st);
+    snaps.push_back(p);
+  }
+  auto restore = [&]() {
+    for (size_t j = 0; j < e->jobs.size() && j < snaps.size(); ++j) {
+      const DevJob &J = e->jobs[j].dj;
+      unsigned char *b = (unsigned char *)snaps[j];
+      cudaMemcpyAsync(J.rep, b, sizeof(ReplicaMC) * J.nrep, cudaMemcpyDeviceToDevice, e->st);
+      cudaMemcpyAsync(J.run_acc, b + sizeof(ReplicaMC) * J.nrep, sizeof(int) * J.nrep, cudaMemcpyDeviceToDevice, e->st);
+      cudaMemcpyAsync(J.stats, b + (sizeof(ReplicaMC) + sizeof(int)) * J.nrep, sizeof(RepStats) * J.nrep,
+                      cudaMemcpyDeviceToDevice, e->st);
+    }
+  };
+  std::string rep;
+  TileConfig best = e->tc;
+  double best_t = 1e300;
+  const int shapes[][2] = {{1, 8}, {2, 4}, {2, 8}, {4, 4}};
+  const int warps[] = {4, 6, 8, 10, 12, 14, 16};
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  for (const auto &sh : shapes) {
+    if (e->precision == GD_PREC_FP64 && !(sh[0] == 1 && sh[1] == 8)) continue;
+    for (int w : warps) {
+      if (rc != GD_OK) break;
+      TileConfig tc{w, sh[0], sh[1]};
+      if (configure(e, tc) != GD_OK) continue;
+      float t = 0;
+      cudaEventRecord(a, e->st);
+      rc = launch_mc(e, e->step, steps, 0);
+      cudaEventRecord(b, e->st);
+      if (cudaStreamSynchronize(e->st) != cudaSuccess) rc = fail(GD_E_CUDA, "autotune launch");
+      cudaEventElapsedTime(&t, a, b);
+      restore();
+      char line[160];
+      snprintf(line, sizeof line, "warps=%d kpl=%d ab=%d grid=%d items=%d: %.3f ms\n", w, sh[0], sh[1], e->grid,
+               e->n_items, t);
+      rep += line;
+      if (t < best_t) {
+        best_t = t;
+        best = tc;
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamSynchronize(e->st);
+  for (void *p : snaps) cudaFree(p);
+  e->ev_used = 0;
+  e->launches = 0;
+  if (rc == GD_OK) rc = configure(e, best);
+  char line[160];
+  snprintf(line, sizeof line, "chosen: warps=%d kpl=%d ab=%d\n", best.warps_per_cta, best.kpl, best.ab);
+  rep += line;
+  if (report && report_len > 0) {
+    std::strncpy(report, rep.c_str(), (size_t)report_len - 1);
+    report[report_len - 1] = 0;
+  }
+  return rc;
+}
+
+int gd_ensemble_destroy(gd_ensemble_t *e)
+{
+  destroy(e);
+  return GD_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- layout --
+// Sizes and offsets of the boundary structs, for bindings that mirror them.
+extern "C" long long gd_layout(const char *what)
+{
+  if (!what) return -1;
+  const std::string w(what);
+#define GD_L(name, expr) \
+  if (w == name) return (long long)(expr);
+  GD_L("sizeof.Complex", sizeof(Complex))
+  GD_L("sizeof.Record", sizeof(Record))
+  GD_L("sizeof.ReplicaMC", sizeof(ReplicaMC))
+  GD_L("sizeof.EnePara", sizeof(EnePara))
+  GD_L("sizeof.EnePara0", sizeof(EnePara0))
+  GD_L("sizeof.Ligand", sizeof(Ligand))
+  GD_L("sizeof.Protein", sizeof(Protein))
+  GD_L("sizeof.Kde", sizeof(Kde))
+  GD_L("sizeof.Mcs", sizeof(Mcs))
+  GD_L("sizeof.ParaT", sizeof(ParaT))
+  GD_L("Complex.lig", offsetof(Complex, lig))
+  GD_L("Complex.prt", offsetof(Complex, prt))
+  GD_L("Complex.psp", offsetof(Complex, psp))
+  GD_L("Complex.kde", offsetof(Complex, kde))
+  GD_L("Complex.mcs", offsetof(Complex, mcs))
+  GD_L("Complex.enepara", offsetof(Complex, enepara))
+  GD_L("Complex.temp", offsetof(Complex, temp))
+  GD_L("Complex.replica", offsetof(Complex, replica))
+  GD_L("Complex.size", offsetof(Complex, size))
+  GD_L("Complex.mcpara", offsetof(Complex, mcpara))
+  GD_L("Complex.lig_file", offsetof(Complex, lig_file))
+  GD_L("Complex.rep_begin", offsetof(Complex, rep_begin))
+  GD_L("Complex.rep_end", offsetof(Complex, rep_end))
+  GD_L("Complex.signal", offsetof(Complex, signal))
+  GD_L("EnePara.w", offsetof(EnePara, w))
+  GD_L("EnePara.hpl0", offsetof(EnePara, hpl0))
+  GD_L("EnePara.kde2", offsetof(EnePara, kde2))
+  GD_L("Record.next_entry", offsetof(Record, next_entry))
+#undef GD_L
+  return -1;
+}
+
+// ------------------------------------------------------ force field --
+// OptimizeEnepara (src/frontend/util_optimize_soa.C:489-540): the same float
+// operations in the same order, so the tables match the reference bit for bit.
+extern "C" int gd_optimize_enepara(const EnePara0 *e0, EnePara *e)
+{
+  if (!e0 || !e) return fail(GD_E_INVALID, "null argument");
+  std::memset(e, 0, sizeof(EnePara));
+  const float sqrt_2_pi = sqrtf(2.0f * 3.1415926535f);
+  for (int i = 0; i < GD_MAXTP2; ++i)
+    for (int j = 0; j < GD_MAXTP1; ++j) {
+      const float tmp = e0->vdw[j][i][0] * e0->lj[2];
+      e->p1a[i][j] = 2.0f * e0->vdw[j][i][1] * powf(tmp, 9.0f);
+      e->p2a[i][j] = 3.0f * e0->vdw[j][i][1] * powf(tmp, 6.0f);
+    }
+  e->lj0 = e0->lj[0];
+  e->lj1 = e0->lj[1];
+  e->el1 = e0->el[1];
+  e->el0 = e0->el[0];
+  e->a1 = 4.0f - 3.0f * e0->el[0];
+  e->b1 = 2.0f * e0->el[0] - 3.0f;
+  for (int i = 0; i < GD_MAXTP2; ++i)
+    for (int j = 0; j < GD_MAXTP1; ++j) {
+      e->pmf0[i][j] = e0->pmf[j][i][0];
+      e->pmf1[i][j] = e0->pmf[j][i][1];
+      e->hdb0[i][j] = e0->hdb[j][i][0];
+      e->hdb1[i][j] = 1.0f / e0->hdb[j][i][1];
+    }
+  for (int i = 0; i < GD_MAXTP4; ++i) e->hpp[i] = e0->hpp[i];
+  for (int i = 0; i < GD_MAXTP2; ++i) {
+    e->hpl0[i] = e0->hpl[i][0];
+    e->hpl1[i] = e0->hpl[i][1];
+    e->hpl2[i] = logf(1.0f / (e->hpl1[i] * sqrt_2_pi));
+  }
+  e->kde2 = -0.5f / (e0->kde * e0->kde);
+  e->kde3 = powf(e0->kde * sqrt_2_pi, 3.0f);
+  for (int i = 0; i < GD_MAXWEI; ++i) {
+    e->w[i] = e0->w[i];
+    e->a_para[i] = e0->a_para[i];
+    e->b_para[i] = e0->b_para[i];
+  }
+  return GD_OK;
+}

@@ -1,0 +1,172 @@
+// gd_internal.h -- device-side layout of the docking data and kernel entry
+// points shared by the translation units of libgdock.so.
+//
+// The reference keeps everything in one fixed-capacity 6.58 MB Complex blob
+// and lets every CUDA block walk it through the read-only cache
+// (src/backend_gpu/kernel_cuda_l1_montecarlo.cu:142-228).  Here the blob is
+// only the boundary format: it is packed once into compact structure-of-arrays
+// buffers sized to the actual problem:
+//
+//   pocket conformation  pos[P] float4 (x, y, z, ele), aux[P] float2 (hpp_eff, type)
+//                        sorted by point type, padded with inert points
+//   force-field tables   tab4[24][32] float4 (p1a, p2a, pmf0, pmf1)
+//                        tab2[24][32] float2 (hdb0, hdb1), unused pairs zeroed
+//   ligand conformation  lig[L] float4 (x, y, z, charge), atoms grouped by type
+//   KDE points           kde[K] float4 (x, y, z, type), sorted by type, with
+//                        per-type ranges
+//   MCS templates        mcs[L][M] float4 (x, y, z, valid), atom-major
+//   pocket potential     psp[prt conf][24][P] pre-gathered per sorted point
+//
+// Every array a CTA stages into shared memory is a multiple of 16 bytes and
+// starts 16-byte aligned, so it can be copied with one 1-D bulk (TMA) copy.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gdock_types.h"
+
+namespace gd {
+
+constexpr int kLigTypes = GD_MAXTP2;     // 24 ligand atom types
+constexpr int kTabCols = 32;             // point-type columns (30 used, 30 = inert padding)
+constexpr int kPadType = 30;             // point type given to padding points
+constexpr int kMaxAtoms = 128;           // ligand atoms per job on the batched path
+constexpr int kPointAlign = 128;         // pocket conformations padded to this many points
+constexpr int kMaxTemps = GD_MAX_TMP;
+constexpr int kMaxCtaThreads = 512;       // launch bound of the batched kernel (<= 16 replica-warps)
+
+// Force-field parameters of one job, in the order the kernels stage them.
+struct alignas(16) DevParams {
+  float4 tab4[kLigTypes][kTabCols];   // p1a, p2a, pmf0, pmf1
+  float2 tab2[kLigTypes][kTabCols];   // hdb0, hdb1 (both 0 where hdb0 <= 0.1)
+  float hpl0[kLigTypes], hpl1[kLigTypes], hpl2[kLigTypes];
+  float a_para[12], b_para[12], w[12];
+  float lj0, lj1, el0, el1, inv_el1, a1, b1, kde2, kde3_inv;
+  float move_scale[6];
+  float pad_[1];
+};
+static_assert(sizeof(DevParams) % 16 == 0, "DevParams must be a multiple of 16 bytes");
+
+// Per-replica running statistics, accumulated on the device in FP64.
+struct alignas(16) RepStats {
+  double e_sum;          // sum of the accepted-state total energy, one sample per step
+  double e_sum2;         // sum of squares
+  double best_e;         // lowest total energy seen
+  long long n_steps;     // steps taken
+  long long n_accept;    // accepted moves
+  long long n_exch_try;  // exchange attempts involving this replica
+  long long n_exch_acc;  // accepted exchanges
+  float best_mm[6];      // pose of best_e
+  int best_step;
+  int pad_;
+};
+
+// One docking job: one ligand (all its conformations) against one pocket.
+struct DevJob {
+  // ligand
+  int natom;               // L
+  int nlig;                // ligand conformations
+  int lstride;             // float4 stride between ligand conformations (>= L)
+  const float4 *lig;       // [nlig][lstride] (x, y, z, charge), type-grouped order
+  const int *ltype;        // [L] atom type in type-grouped order
+  const float *lcenter;    // [nlig][3] ligand centre in the lab frame
+  // pocket
+  int npoint_pad;          // padded point count (multiple of kPointAlign)
+  int nprt;                // protein conformations
+  const float4 *pos;       // [nprt][npoint_pad]
+  const float2 *aux;       // [nprt][npoint_pad]
+  const float *pcenter;    // [nprt][3] pocket centre
+  const float *psp;        // [nprt][24][npoint_pad]
+  // KDE
+  int nkde;
+  const float4 *kde;       // [nkde]
+  int kbeg[kLigTypes];
+  int kcnt[kLigTypes];
+  // MCS
+  int nmcs;
+  const float4 *mcs;       // [L][nmcs]
+  const float *tcc;        // [nmcs]
+  // temperatures
+  int ntmp;
+  const float *minus_beta; // [ntmp]
+  // parameters
+  const DevParams *par;
+  // replicas (layout of the reference's replica array: index
+  // n_tmp*n_lig*p + n_lig*t + l, src/frontend/util.C:380)
+  int nrep;
+  ReplicaMC *rep;          // [nrep]
+  int *run_acc;            // [nrep] accept flag of the last step
+  RepStats *stats;         // [nrep]
+  Record *rec;             // [nrep] or nullptr
+  uint32_t key0, key1;     // Philox key (job seed)
+  int rid_base;            // global index of local replica 0 (Philox counter, exchange partners)
+  int nrep_total;          // replicas of the whole ensemble (nlig * nprt * ntmp)
+};
+
+// One unit of work of the batched kernel: `count` consecutive replicas of
+// one job that share protein conformation `prt`.
+struct WorkItem {
+  int job;
+  int prt;
+  int rep0;
+  int count;
+};
+
+// Kernel configuration chosen by the autotuner.
+struct TileConfig {
+  int warps_per_cta;   // replicas per CTA (one warp each)
+  int kpl;             // pocket points per lane per row (1, 2 or 4)
+  int ab;              // ligand atoms per register block (4 or 8)
+};
+
+enum Precision { kFP32 = 0, kFP32Kahan = 1, kFP64 = 2 };
+
+// Launch flags of the Monte Carlo kernels.
+enum McFlags {
+  kMcRecord = 1,         // append accepted states to Record
+  kMcResetRecord = 2,    // this launch starts a dump chunk (next_entry = 0)
+  kMcStoreAccept = 4,    // write the running accept flag into ReplicaMC.is_accept at the end
+  kMcInitial = 8,        // initial-energy evaluation: no move, forced accept
+};
+
+// Error flags written by kernels into a device word.
+enum DevError { kErrNone = 0, kErrTimeout = 1, kErrSize = 2 };
+
+// ---- kernels (gd_mc.cu) ----------------------------------------------------
+
+// Arguments of the batched kernel (Monte Carlo mode and pose-evaluation mode).
+struct KArgs {
+  const DevJob *jobs;
+  const WorkItem *items;
+  int n_items;
+  int *queue;
+  int *err;
+  int s_begin, nsteps, flags;
+  int P, Kst, lig_slots;   // smem layout parameters (maximum over the launched jobs)
+  // pose evaluation
+  const int *conf;
+  const float *mm;
+  float *out;
+  double *out64;
+  float *raw;
+};
+
+// Shared-memory bytes of the batched kernel for pocket conformations of P
+// points, Kst KDE points staged, lig_slots ligand atoms and `warps` replicas per CTA.
+size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision);
+
+// Resident CTAs per SM of the batched kernel for this configuration (0 if it cannot launch).
+int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem);
+
+// mode 0: Monte Carlo chunk over the work items; mode 1: pose evaluation.
+cudaError_t launch_kernel(int mode, int precision, const TileConfig &tc, const KArgs &a, int grid, cudaStream_t st);
+
+// Replica-exchange sweep x of one job (ngroup = nprt * nlig groups of ntmp temperatures).
+cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cudaStream_t st);
+
+// The plain kernel (gd_plain.cu): one CTA per replica, the reference's launch structure.
+cudaError_t launch_plain(const DevJob *d_job, int nrep, int s_begin, int nsteps, int flags, int *d_err,
+                         cudaStream_t st);
+
+}  // namespace gd

@@ -1,0 +1,690 @@
+// gd_mc.cu -- the batched Monte Carlo kernel (one warp per replica), the
+// pose-evaluation kernel that shares its energy code, and the replica
+// exchange kernel.
+//
+// Mapping to the hardware.  The reference runs one 1024-thread block per
+// replica and synchronises the block six or more times per step
+// (src/backend_gpu/kernel_cuda_l1_montecarlo.cu:284-527).  Here one warp owns
+// one replica for a whole chunk of steps: the step needs no block barrier,
+// only warp shuffles.  A CTA holds R replica-warps that share one protein
+// conformation; the CTA stages that conformation, the KDE points and the
+// force-field tables into shared memory with 1-D bulk (TMA) copies once per
+// work item, and the replica-warps then read them for every step.
+//
+// Pair loop.  Lane i owns pocket points row+i+32j (j < KPL) in registers and
+// walks the ligand atoms (grouped by atom type) in blocks of AB atoms, so each
+// point is loaded from shared memory once per AB atoms, the per-(atom type,
+// point type) table entries are reloaded only when the atom type changes, and
+// the per-atom hydrophobic sums stay in registers until one warp reduction
+// per atom.  Pocket points are sorted by point type, so neighbouring lanes
+// read the same table entries (shared-memory broadcast).
+//
+// Arithmetic follows src/backend_gpu/energy_prt_v1.cu:8-174 term by term; the
+// special functions use the single-instruction PTX approximations
+// (rsqrt/rcp/ex2.approx) and powers of 1/d by multiplication.  The
+// FP32-Kahan variant adds each (atom block x point row) partial sum into the
+// lane totals with compensated summation and reduces across lanes with a
+// compensated butterfly; the FP64 variant does the pair arithmetic in double.
+#include <cstdio>
+#include <type_traits>
+
+#include "gd_device.cuh"
+#include "gd_internal.h"
+
+namespace gd {
+
+namespace {
+
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kSqrt2PiInvNeg = -0.3989422804014327f;  // -1/sqrt(2 pi), kernel_cuda_l1_montecarlo.cu:14
+constexpr uint32_t kWaitLimit = 1u << 26;
+
+// hydrophobic contact polynomial 1 - (3.5/81 d2 - 4.5/81^2 d4 + 2.5/81^3 d6 - 0.5/81^4 d8)
+// (energy_prt_v1.cu:44-48), in Horner form in d2
+constexpr double kH1 = -3.5 / 81.0;
+constexpr double kH2 = 4.5 / (81.0 * 81.0);
+constexpr double kH3 = -2.5 / (81.0 * 81.0 * 81.0);
+constexpr double kH4 = 0.5 / (81.0 * 81.0 * 81.0 * 81.0);
+
+template <typename T>
+struct alignas(16) V4 {
+  T x, y, z, w;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+}  // namespace
+
+// ----------------------------------------------------------- smem layout --
+struct SmemLayout {
+  uint32_t params, ltype, pos, aux, kde, warp0, warp_bytes, lig_bytes, total;
+};
+
+__host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots, int warps, bool fp64)
+{
+  SmemLayout s;
+  uint32_t off = 0;
+  s.params = off;
+  off = align16(off + (uint32_t)sizeof(DevParams));
+  s.ltype = off;
+  off = align16(off + (uint32_t)sizeof(int) * kMaxAtoms);
+  s.pos = off;
+  off = align16(off + 16u * (uint32_t)P);
+  s.aux = off;
+  off = align16(off + 8u * (uint32_t)P);
+  s.kde = off;
+  off = align16(off + 16u * (uint32_t)Kst);
+  s.lig_bytes = (uint32_t)lig_slots * (fp64 ? 32u : 16u);
+  // per warp: rotated ligand, ReplicaMC state, EnergyScratch (192 B), WarpStats (64 B)
+  s.warp_bytes = align16(s.lig_bytes + (uint32_t)sizeof(ReplicaMC) + 192u + 64u);
+  s.warp0 = off;
+  off += s.warp_bytes * (uint32_t)warps;
+  s.total = off;
+  return s;
+}
+
+// ------------------------------------------------------------- energy --
+// Energy of ligand conformation ilig at pose mm in protein conformation iprt.
+// Called by all 32 lanes of a warp; on return every lane holds e[0..9]
+// (normalised terms and total) and raw[0..8] (terms before normalisation).
+// Per-warp results of energy_warp (written by lane 0 after the reductions).
+struct EnergyScratch {
+  double e[10];    // normalised terms and total
+  double raw[9];   // terms before the per-atom division and normalisation
+  float mm[6];     // pose being evaluated (input)
+  float pad_[4];
+};
+static_assert(sizeof(EnergyScratch) == 192, "EnergyScratch size is part of the smem layout");
+
+template <int PREC, int KPL, int AB>
+__device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__restrict__ par,
+                                         const float4 *__restrict__ pos, const float2 *__restrict__ aux,
+                                         const float4 *__restrict__ kde, const int *__restrict__ ltype, void *ligbuf,
+                                         int ilig, int iprt, const float *mm, EnergyScratch *out)
+{
+  using T = typename std::conditional<PREC == kFP64, double, float>::type;
+  const int lane = lane_id();
+  const int L = J.natom;
+  const int P = J.npoint_pad;
+  V4<T> *lig = reinterpret_cast<V4<T> *>(ligbuf);
+
+  // rotation + translation, kernel_cuda_l1_montecarlo.cu:336-380
+  T r00, r01, r02, r10, r11, r12, r20, r21, r22;
+  {
+    T s1, c1, s2, c2, s3, c3;
+    if constexpr (PREC == kFP64) {
+      sincos((double)mm[3], &s1, &c1);
+      sincos((double)mm[4], &s2, &c2);
+      sincos((double)mm[5], &s3, &c3);
+    } else {
+      sincosf(mm[3], &s1, &c1);
+      sincosf(mm[4], &s2, &c2);
+      sincosf(mm[5], &s3, &c3);
+    }
+    r00 = c1 * c2;
+    r01 = c1 * s2 * s3 - c3 * s1;
+    r02 = s1 * s3 + c1 * c3 * s2;
+    r10 = c2 * s1;
+    r11 = c1 * c3 + s1 * s2 * s3;
+    r12 = c3 * s1 * s2 - c1 * s3;
+    r20 = -s2;
+    r21 = c2 * s3;
+    r22 = c2 * c3;
+  }
+  const float *lc = J.lcenter + 3 * ilig;
+  const T tx = (T)mm[0] + (T)lc[0], ty = (T)mm[1] + (T)lc[1], tz = (T)mm[2] + (T)lc[2];
+  const float4 *lsrc = J.lig + (size_t)ilig * J.lstride;
+  for (int a = lane; a < L; a += 32) {
+    const float4 v = lsrc[a];
+    V4<T> o;
+    o.x = r00 * (T)v.x + r01 * (T)v.y + r02 * (T)v.z + tx;
+    o.y = r10 * (T)v.x + r11 * (T)v.y + r12 * (T)v.z + ty;
+    o.z = r20 * (T)v.x + r21 * (T)v.y + r22 * (T)v.z + tz;
+    o.w = (T)v.w;
+    lig[a] = o;
+  }
+  __syncwarp();
+
+  // ---- protein-ligand pair terms, energy_prt_v1.cu:8-174
+  const T lj0 = par->lj0, lj1 = par->lj1, el0 = par->el0, el1 = par->el1, inv_el1 = par->inv_el1;
+  const T a1 = par->a1, b1 = par->b1;
+  T s_vdw = 0, s_ele = 0, s_pmf = 0, s_psp = 0, s_hdb = 0;
+  float c_vdw = 0.f, c_ele = 0.f, c_pmf = 0.f, c_psp = 0.f, c_hdb = 0.f;  // Kahan compensations
+  T ehpc = 0;
+  const float *pspc = J.psp + (size_t)iprt * kLigTypes * P;
+
+  for (int a0 = 0; a0 < L; a0 += AB) {
+    T hpc[AB];
+#pragma unroll
+    for (int k = 0; k < AB; ++k) hpc[k] = 0;
+
+    for (int row = 0; row < P; row += 32 * KPL) {
+      T px[KPL], py[KPL], pz[KPL], pe[KPL], ph[KPL];
+      int pt[KPL];
+#pragma unroll
+      for (int j = 0; j < KPL; ++j) {
+        const int p = row + 32 * j + lane;
+        const float4 q = pos[p];
+        const float2 w = aux[p];
+        px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
+        ph[j] = w.x;
+        pt[j] = __float_as_int(w.y);
+      }
+      T t_p1a[KPL], t_p2a[KPL], t_pmf0[KPL], t_pmf1[KPL], t_hdb0[KPL], t_hdb1[KPL], t_psp[KPL];
+      int cur = -1;
+      T b_vdw = 0, b_ele = 0, b_pmf = 0, b_psp = 0, b_hdb = 0;
+
+#pragma unroll
+      for (int k = 0; k < AB; ++k) {
+        const int a = a0 + k;
+        if (a >= L) break;
+        const V4<T> la = lig[a];
+        const int lt = ltype[a];
+        if (lt != cur) {
+          cur = lt;
+#pragma unroll
+          for (int j = 0; j < KPL; ++j) {
+            const float4 t4 = par->tab4[lt][pt[j]];
+            const float2 t2 = par->tab2[lt][pt[j]];
+            t_p1a[j] = t4.x; t_p2a[j] = t4.y; t_pmf0[j] = t4.z; t_pmf1[j] = t4.w;
+            t_hdb0[j] = t2.x; t_hdb1[j] = t2.y;
+            t_psp[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+          const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
+          const T d2 = dx * dx + dy * dy + dz * dz;
+          T r;
+          if constexpr (PREC == kFP64) r = rsqrt(d2);
+          else r = rsqrt_approx(d2);
+          const T d = d2 * r;
+
+          // hydrophobic contact (cdc == 1 folded into hpp_eff), energy_prt_v1.cu:42-49
+          const T poly = (((T)kH4 * d2 + (T)kH3) * d2 + (T)kH2) * d2 + (T)kH1;
+          const T hp = poly * d2 + (T)1;
+          hpc[k] += (d2 <= (T)81) ? ph[j] * hp : (T)0;
+
+          // Lennard-Jones, energy_prt_v1.cu:60-63: p1 = p1a/d^9, p2 = p2a/d^6
+          const T r2 = r * r;
+          const T r3 = r2 * r;
+          const T r6 = r3 * r3;
+          const T p1 = t_p1a[j] * (r6 * r3);
+          const T p2 = t_p2a[j] * r6;
+          const T p4 = p1 * lj0 * ((T)1 + lj1 * d2) + (T)1;
+          T inv_p4;
+          if constexpr (PREC == kFP64) inv_p4 = 1.0 / p4;
+          else inv_p4 = rcp_approx(p4);
+          b_vdw += (p1 - p2) * inv_p4;
+
+          // electrostatics, energy_prt_v1.cu:81-85
+          const T s1 = el1 * d;
+          const T g_near = el0 + s1 * s1 * (a1 + b1 * s1);
+          const T g_far = r * inv_el1;
+          const T g1 = (s1 < (T)1) ? g_near : g_far;
+          b_ele += la.w * pe[j] * g1;
+
+          // contact (pmf) sigmoid, energy_prt_v1.cu:95-97
+          const T dmp = d - t_pmf0[j];
+          T ex, inv_den;
+          if constexpr (PREC == kFP64) {
+            ex = exp((-0.5 * d + 6.0) * dmp);
+            inv_den = 1.0 / (1.0 + ex);
+          } else {
+            ex = ex2_approx(((-0.5f * kLog2e) * d + 6.0f * kLog2e) * dmp);
+            inv_den = rcp_approx(1.0f + ex);
+          }
+          b_pmf += t_pmf1[j] * inv_den;
+
+          // pocket-specific potential (c == 2 folded into t_psp), energy_prt_v1.cu:109-115
+          b_psp += (dmp <= (T)0) ? t_psp[j] : (T)0;
+
+          // hydrogen bond (hdb0 <= 0.1 folded into hdb1 = 0), energy_prt_v1.cu:133-138
+          const T h3 = (d - t_hdb0[j]) * t_hdb1[j];
+          T g;
+          if constexpr (PREC == kFP64) g = exp(-0.5 * h3 * h3);
+          else g = ex2_approx((-0.5f * kLog2e) * h3 * h3);
+          b_hdb += t_hdb1[j] * g;
+        }
+      }
+      if constexpr (PREC == kFP32Kahan) {
+        kahan_add(s_vdw, c_vdw, b_vdw);
+        kahan_add(s_ele, c_ele, b_ele);
+        kahan_add(s_pmf, c_pmf, b_pmf);
+        kahan_add(s_psp, c_psp, b_psp);
+        kahan_add(s_hdb, c_hdb, b_hdb);
+      } else {
+        s_vdw += b_vdw;
+        s_ele += b_ele;
+        s_pmf += b_pmf;
+        s_psp += b_psp;
+        s_hdb += b_hdb;
+      }
+    }
+    // hydrophobic restraint per atom, energy_prt_v1.cu:162-169
+#pragma unroll
+    for (int k = 0; k < AB; ++k) {
+      const int a = a0 + k;
+      if (a >= L) break;
+      const T S = warp_sum(hpc[k]);
+      const int lt = ltype[a];
+      const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
+      ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
+    }
+  }
+
+  T vdw, ele, pmf, psp, hdb;
+  if constexpr (PREC == kFP32Kahan) {
+    vdw = warp_sum_comp(s_vdw, c_vdw);
+    ele = warp_sum_comp(s_ele, c_ele);
+    pmf = warp_sum_comp(s_pmf, c_pmf);
+    psp = warp_sum_comp(s_psp, c_psp);
+    hdb = warp_sum_comp(s_hdb, c_hdb);
+  } else {
+    vdw = warp_sum(s_vdw);
+    ele = warp_sum(s_ele);
+    pmf = warp_sum(s_pmf);
+    psp = warp_sum(s_psp);
+    hdb = warp_sum(s_hdb);
+  }
+
+  // ---- KDE, energy_kde_v1.cu:183-274: per atom, mean of exp(kde2 d^2) over
+  // the KDE points of the same type; atoms with no such point contribute 0.
+  T kacc = 0;
+  {
+    const T kde2 = par->kde2;
+    for (int a = 0; a < L; ++a) {
+      const int lt = ltype[a];
+      const int cnt = J.kcnt[lt];
+      if (cnt == 0) continue;
+      const int beg = J.kbeg[lt];
+      const V4<T> la = lig[a];
+      const T inv = (T)1 / (T)cnt;
+      for (int k = beg + lane; k < beg + cnt; k += 32) {
+        const float4 q = kde[k];
+        const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+        const T d2 = dx * dx + dy * dy + dz * dz;
+        if constexpr (PREC == kFP64) kacc += exp(kde2 * d2) * inv;
+        else kacc += ex2_approx((kde2 * kLog2e) * d2) * inv;
+      }
+    }
+  }
+  const T ekde = warp_sum(kacc) * (T)par->kde3_inv;
+
+  // ---- MCS, energy_mcs_v1.cu:277-320
+  T macc = 0;
+  {
+    const int M = J.nmcs;
+    for (int m0 = 0; m0 < M; m0 += 32) {
+      const int m = m0 + lane;
+      if (m < M) {
+        T s = 0;
+        int n = 0;
+        for (int a = 0; a < L; ++a) {
+          const float4 q = J.mcs[(size_t)a * M + m];
+          if (q.w != 0.0f) {
+            const V4<T> la = lig[a];
+            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+            s += dx * dx + dy * dy + dz * dz;
+            ++n;
+          }
+        }
+        macc += (T)J.tcc[m] * sqrt(s / (T)n);
+      }
+    }
+  }
+  const T elhm = warp_sum(macc);
+
+  // ---- distance to the pocket centre, kernel_cuda_l1_montecarlo.cu:439-454
+  const float *pc = J.pcenter + 3 * iprt;
+  T dst = 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const T t = ((T)lc[i] + (T)mm[i]) - (T)pc[i];
+    dst += t * t;
+  }
+
+  T r9[9];
+  r9[0] = vdw;
+  r9[1] = ele;
+  r9[2] = pmf;
+  r9[3] = psp;
+  r9[4] = hdb * (T)kSqrt2PiInvNeg;
+  r9[5] = ehpc;
+  r9[6] = ekde;
+  r9[7] = log(elhm / (T)J.nmcs);
+  r9[8] = sqrt(dst);
+
+  // normalisation and weighted total, kernel_cuda_l1_montecarlo.cu:460-476
+  if (lane == 0) {
+    T tot = 0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      out->raw[i] = (double)r9[i];
+      T v = r9[i];
+      if (i < 7) v = v / (T)L;
+      v = (T)par->a_para[i] * v + (T)par->b_para[i];
+      out->e[i] = (double)v;
+      tot += (T)par->w[i] * v;
+    }
+    out->e[9] = (double)tot;
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------ kernels --
+
+
+// Stage the shared data of work item `wi` into shared memory.  Returns false
+// if the bulk copies did not complete within the wait limit.
+template <bool FP64>
+__device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, unsigned char *smem,
+                           const SmemLayout &sl, uint64_t *bar, uint32_t &phase)
+{
+  const int P = J.npoint_pad;
+  const bool kde_in_smem = J.nkde <= A.Kst;
+  if (threadIdx.x == 0) {
+    fence_proxy_async_smem();
+    uint32_t bytes = (uint32_t)sizeof(DevParams) + 24u * (uint32_t)P;
+    if (kde_in_smem) bytes += 16u * (uint32_t)J.nkde;
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(smem + sl.params, J.par, (uint32_t)sizeof(DevParams), bar);
+    bulk_g2s(smem + sl.pos, J.pos + (size_t)wi.prt * P, 16u * (uint32_t)P, bar);
+    bulk_g2s(smem + sl.aux, J.aux + (size_t)wi.prt * P, 8u * (uint32_t)P, bar);
+    if (kde_in_smem && J.nkde > 0) bulk_g2s(smem + sl.kde, J.kde, 16u * (uint32_t)J.nkde, bar);
+  }
+  int *lt = reinterpret_cast<int *>(smem + sl.ltype);
+  for (int a = threadIdx.x; a < J.natom; a += blockDim.x) lt[a] = J.ltype[a];
+  const bool ok = mbar_wait(bar, phase, kWaitLimit);
+  phase ^= 1u;
+  return ok;
+}
+
+// Per-warp FP64 statistics kept in shared memory during a chunk (lane 0).
+struct WarpStats {
+  double e_sum, e_sum2, best_e;
+  long long n_acc;
+  float best_mm[6];
+  int best_step;
+  int pad_;
+};
+
+template <int MODE, int PREC, int KPL, int AB>
+__global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_item;
+  const SmemLayout sl = smem_layout(A.P, A.Kst, A.lig_slots, blockDim.x / 32, PREC == kFP64);
+  const int warp = threadIdx.x >> 5;
+  const int lane = lane_id();
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  uint32_t phase = 0;
+  int prev_job = -1, prev_prt = -1;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= A.n_items) break;
+    const WorkItem wi = A.items[it];
+    const DevJob &J = A.jobs[wi.job];
+    if (wi.job != prev_job || wi.prt != prev_prt) {
+      if (!stage_item<PREC == kFP64>(A, J, wi, smem, sl, &bar, phase)) {
+        if (threadIdx.x == 0) atomicOr(A.err, kErrTimeout);
+        mbar_wait(&bar, phase ^ 1u, kWaitLimit);  // let the copies in flight land before exiting
+        return;
+      }
+      prev_job = wi.job;
+      prev_prt = wi.prt;
+    }
+    __syncthreads();
+
+    const DevParams *par = reinterpret_cast<const DevParams *>(smem + sl.params);
+    const float4 *pos = reinterpret_cast<const float4 *>(smem + sl.pos);
+    const float2 *aux = reinterpret_cast<const float2 *>(smem + sl.aux);
+    const float4 *kde = (J.nkde <= A.Kst) ? reinterpret_cast<const float4 *>(smem + sl.kde) : J.kde;
+    const int *ltype = reinterpret_cast<const int *>(smem + sl.ltype);
+    unsigned char *wbase = smem + sl.warp0 + (size_t)warp * sl.warp_bytes;
+    void *ligbuf = wbase;
+    ReplicaMC *srep = reinterpret_cast<ReplicaMC *>(wbase + sl.lig_bytes);
+    EnergyScratch *esc = reinterpret_cast<EnergyScratch *>(wbase + sl.lig_bytes + sizeof(ReplicaMC));
+    WarpStats *wst = reinterpret_cast<WarpStats *>(wbase + sl.lig_bytes + sizeof(ReplicaMC) + sizeof(EnergyScratch));
+
+    if (warp < wi.count) {
+      const int r = wi.rep0 + warp;  // job-local index
+      if constexpr (MODE == 1) {
+        // ---- pose evaluation
+        const int ilig = A.conf[2 * r], iprt = A.conf[2 * r + 1];
+        if (lane < 6) esc->mm[lane] = A.mm[6 * r + lane];
+        __syncwarp();
+        energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, ltype, ligbuf, ilig, iprt, esc->mm, esc);
+        if (lane < 10) {
+          A.out[10 * (size_t)r + lane] = (float)esc->e[lane];
+          if (A.out64) A.out64[10 * (size_t)r + lane] = esc->e[lane];
+        }
+        if (A.raw && lane < 9) A.raw[9 * (size_t)r + lane] = (float)esc->raw[lane];
+        __syncwarp();
+      } else {
+        // ---- Monte Carlo chunk for replica r
+        const int gr = J.rid_base + r;
+        int *sw = reinterpret_cast<int *>(srep);
+        sw[lane] = reinterpret_cast<const int *>(J.rep + r)[lane];
+        if (lane == 0) {
+          const RepStats &S = J.stats[r];
+          wst->e_sum = 0.0;
+          wst->e_sum2 = 0.0;
+          wst->n_acc = 0;
+          wst->best_e = S.best_e;
+          wst->best_step = S.best_step;
+          for (int i = 0; i < 6; ++i) wst->best_mm[i] = S.best_mm[i];
+        }
+        __syncwarp();
+        int acc = J.run_acc[r];
+        const int ilig = srep->idx_lig, iprt = srep->idx_prt;
+        const double mbeta = (double)J.minus_beta[srep->idx_tmp];
+        Record *rec = (J.rec && (A.flags & kMcRecord)) ? J.rec + r : nullptr;
+        int ne = 0;
+        if (J.rec && (A.flags & kMcResetRecord)) {
+          if (lane == 0) J.rec[r].next_entry = 0;
+        } else if (rec) {
+          ne = rec->next_entry;
+        }
+        const bool initial = (A.flags & kMcInitial) != 0;
+
+        for (int s = A.s_begin; s < A.s_begin + A.nsteps; ++s) {
+          if (acc) {
+            // record the old state, kernel_cuda_l1_montecarlo.cu:290-297
+            if (lane == 0) srep->step = s;
+            __syncwarp();
+            if (rec && ne < GD_STEPS_PER_DUMP) reinterpret_cast<int *>(&rec->replica[ne])[lane] = sw[lane];
+            ++ne;
+          }
+          // draws of step s: counter {s, replica, 0, 0} -> move x y z, rot x;
+          // {s, replica, 0, 1} -> rot y z, accept (lane 0 and lane 1 compute one each)
+          float u_acc = 0.0f;
+          if (!initial) {
+            const Philox4 d = philox4x32_10((uint32_t)s, (uint32_t)gr, 0u, (uint32_t)(lane & 1), J.key0, J.key1);
+            float u[7];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) u[k] = u01(__shfl_sync(0xffffffffu, d.v[k], 0));
+#pragma unroll
+            for (int k = 4; k < 7; ++k) u[k] = u01(__shfl_sync(0xffffffffu, d.v[k - 4], 1));
+            u_acc = u[6];
+            if (lane < 6) {
+              float v = u[0];
+#pragma unroll
+              for (int i = 1; i < 6; ++i) v = (lane == i) ? u[i] : v;
+              esc->mm[lane] = __fmaf_rn(par->move_scale[lane], v, srep->movematrix[lane]);
+            }
+          } else if (lane < 6) {
+            esc->mm[lane] = __fmaf_rn(par->move_scale[lane], 0.0f, srep->movematrix[lane]);
+          }
+          __syncwarp();
+          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, ltype, ligbuf, ilig, iprt, esc->mm, esc);
+          const float etot = (float)esc->e[9];
+
+          // Metropolis test in FP64, kernel_cuda_l1_montecarlo.cu:485-507
+          int accept = 1;
+          if (!initial) {
+            const double lr = ((double)etot - (double)srep->energy[9]) * mbeta;
+            accept = log((double)u_acc) < lr;
+          }
+          __syncwarp();
+          if (accept) {
+            if (lane < 10) srep->energy[lane] = (float)esc->e[lane];
+            if (lane < 6) srep->movematrix[lane] = esc->mm[lane];
+          }
+          __syncwarp();
+          if (lane == 0) {
+            const double ecur = (double)srep->energy[9];
+            wst->n_acc += accept;
+            wst->e_sum += ecur;
+            wst->e_sum2 += ecur * ecur;
+            if (wst->best_step < 0 || ecur < wst->best_e) {
+              wst->best_e = ecur;
+              wst->best_step = s;
+              for (int i = 0; i < 6; ++i) wst->best_mm[i] = srep->movematrix[i];
+            }
+          }
+          acc = accept;
+        }
+
+        if (lane == 0) {
+          J.run_acc[r] = acc;
+          if (A.flags & kMcStoreAccept) srep->is_accept = acc;
+          if (rec) rec->next_entry = ne;
+          RepStats &S = J.stats[r];
+          S.e_sum += wst->e_sum;
+          S.e_sum2 += wst->e_sum2;
+          S.n_steps += A.nsteps;
+          S.n_accept += wst->n_acc;
+          S.best_e = wst->best_e;
+          S.best_step = wst->best_step;
+          for (int i = 0; i < 6; ++i) S.best_mm[i] = wst->best_mm[i];
+        }
+        __syncwarp();
+        reinterpret_cast<int *>(J.rep + r)[lane] = sw[lane];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Replica exchange between adjacent temperatures.  Sweep x pairs (t, t+1) for
+// t = x mod 2, x mod 2 + 2, ... in every (protein conf p, ligand conf l)
+// group; replica index n_tmp*n_lig*p + n_lig*t + l (src/frontend/util.C:380).
+__global__ void exchange_kernel(const DevJob *jobp, int x)
+{
+  const DevJob &J = *jobp;
+  const int npair = (J.ntmp - (x & 1)) / 2;
+  if (npair <= 0) return;
+  const int ngroup = J.nprt * J.nlig;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= ngroup * npair) return;
+  const int g = tid / npair, i = tid % npair;
+  const int p = g / J.nlig, l = g % J.nlig;
+  const int t = (x & 1) + 2 * i;
+  const int ga = J.ntmp * J.nlig * p + J.nlig * t + l;
+  const int gb = ga + J.nlig;
+  const int ra = ga - J.rid_base, rb = gb - J.rid_base;
+  if (ra < 0 || rb >= J.nrep) return;
+  ReplicaMC *A = J.rep + ra, *B = J.rep + rb;
+  const Philox4 d = philox4x32_10((uint32_t)x, (uint32_t)g, 1u, (uint32_t)t, J.key0, J.key1);
+  const double u = (double)u01(d.v[0]);
+  const double ba = -(double)J.minus_beta[t], bb = -(double)J.minus_beta[t + 1];
+  const double lr = (ba - bb) * ((double)A->energy[9] - (double)B->energy[9]);
+  J.stats[ra].n_exch_try += 1;
+  J.stats[rb].n_exch_try += 1;
+  if (log(u) < lr) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      const float tmp = A->energy[k];
+      A->energy[k] = B->energy[k];
+      B->energy[k] = tmp;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float tmp = A->movematrix[k];
+      A->movematrix[k] = B->movematrix[k];
+      B->movematrix[k] = tmp;
+    }
+    J.run_acc[ra] = 1;
+    J.run_acc[rb] = 1;
+    J.stats[ra].n_exch_acc += 1;
+    J.stats[rb].n_exch_acc += 1;
+  }
+}
+
+// ---------------------------------------------------------- launchers --
+size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision)
+{
+  return smem_layout(P, Kst, lig_slots, warps, precision == kFP64).total;
+}
+
+template <int MODE, int PREC, int KPL, int AB>
+static cudaError_t launch_t(const KArgs &a, int warps, int grid, cudaStream_t st)
+{
+  const size_t smem = kernel_smem_bytes(a.P, a.Kst, a.lig_slots, warps, PREC);
+  auto k = mc_kernel<MODE, PREC, KPL, AB>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, warps * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int MODE, int PREC>
+static cudaError_t launch_p(const KArgs &a, const TileConfig &tc, int grid, cudaStream_t st)
+{
+  const int w = tc.warps_per_cta;
+  if (tc.kpl == 1 && tc.ab == 8) return launch_t<MODE, PREC, 1, 8>(a, w, grid, st);
+  if (tc.kpl == 2 && tc.ab == 4) return launch_t<MODE, PREC, 2, 4>(a, w, grid, st);
+  if (tc.kpl == 2 && tc.ab == 8) return launch_t<MODE, PREC, 2, 8>(a, w, grid, st);
+  if (tc.kpl == 4 && tc.ab == 4) return launch_t<MODE, PREC, 4, 4>(a, w, grid, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_kernel(int mode, int precision, const TileConfig &tc, const KArgs &a, int grid, cudaStream_t st)
+{
+  if (mode == 0) {
+    if (precision == kFP32) return launch_p<0, kFP32>(a, tc, grid, st);
+    if (precision == kFP32Kahan) return launch_p<0, kFP32Kahan>(a, tc, grid, st);
+    if (precision == kFP64) return launch_p<0, kFP64>(a, tc, grid, st);
+  } else {
+    if (precision == kFP32) return launch_p<1, kFP32>(a, tc, grid, st);
+    if (precision == kFP32Kahan) return launch_p<1, kFP32Kahan>(a, tc, grid, st);
+    if (precision == kFP64) return launch_p<1, kFP64>(a, tc, grid, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem)
+{
+  const void *f = nullptr;
+#define GD_PICK(M, PR, K, A)                                                                  \
+  if (mode == M && precision == PR && tc.kpl == K && tc.ab == A) f = (const void *)mc_kernel<M, PR, K, A>;
+#define GD_PICK_ALL(M, PR) GD_PICK(M, PR, 1, 8) GD_PICK(M, PR, 2, 4) GD_PICK(M, PR, 2, 8) GD_PICK(M, PR, 4, 4)
+  GD_PICK_ALL(0, kFP32) GD_PICK_ALL(0, kFP32Kahan) GD_PICK_ALL(0, kFP64)
+  GD_PICK_ALL(1, kFP32) GD_PICK_ALL(1, kFP32Kahan) GD_PICK_ALL(1, kFP64)
+#undef GD_PICK_ALL
+#undef GD_PICK
+  if (!f) return 0;
+  if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, tc.warps_per_cta * 32, smem) != cudaSuccess) return 0;
+  return nb;
+}
+
+cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cudaStream_t st)
+{
+  const int npair = (ntmp - (x & 1)) / 2;
+  if (npair <= 0 || ngroup <= 0) return cudaSuccess;
+  const int n = ngroup * npair;
+  exchange_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_job, x);
+  return cudaGetLastError();
+}
+
+}  // namespace gd

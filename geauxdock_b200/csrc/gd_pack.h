@@ -1,0 +1,101 @@
+// gd_pack.h -- host-side job description and packing into the device layout.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "gd_internal.h"
+#include "gdock.h"
+
+namespace gd {
+
+// Sets the calling thread's error message; returns `code`.
+int fail(int code, const char *fmt, ...);
+
+#define GD_CUDA(call)                                                                                \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return ::gd::fail(GD_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+#define GD_TRY(expr)             \
+  do {                           \
+    const int rc_ = (expr);      \
+    if (rc_ != GD_OK) return rc_; \
+  } while (0)
+
+// Pocket (protein conformations) in dense host arrays.
+struct PocketData {
+  int nconf = 0, P = 0;              // P = max points over conformations
+  std::vector<int> npts;             // [nconf]
+  std::vector<float> xyz;            // [nconf][P][3]
+  std::vector<int> type, cls, cdc, seq3r;  // [nconf][P]
+  std::vector<float> hpp, ele;       // [nconf][P]
+  std::vector<float> center;         // [nconf][3]
+};
+
+// One docking job in dense host arrays.
+struct JobData {
+  int L = 0, nlig = 0;
+  std::vector<float> lxyz;           // [nlig][L][3], ligand-centre frame, input atom order
+  std::vector<int> ltype;            // [L]
+  std::vector<float> lcharge;        // [L]
+  std::vector<float> lcenter;        // [nlig][3]
+  int K = 0;
+  std::vector<float> kxyz;           // [K][3]
+  std::vector<int> ktype;            // [K]
+  int M = 0;
+  std::vector<float> mxyz;           // [M][L][3]
+  std::vector<float> tcc;            // [M]
+  int psp_ncol = 0;
+  std::vector<float> psp;            // [24][psp_ncol]
+  int ntmp = 0;
+  std::vector<float> minus_beta;     // [ntmp]
+  float move_scale[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t seed = 0;
+  int nprt = 0;                      // protein conformations of the pocket
+  std::vector<ReplicaMC> reps;       // replicas to run (a contiguous range)
+  int rid_base = 0;                  // ensemble index of reps[0]
+  int nrep_total = 0;                // nlig * nprt * ntmp
+};
+
+// Device copy of a pocket: type-sorted, padded conformations.
+struct DevPocket {
+  int nconf = 0, Ppad = 0;
+  float4 *pos = nullptr;             // [nconf][Ppad]
+  float2 *aux = nullptr;             // [nconf][Ppad]
+  float *center = nullptr;           // [nconf][3]
+  std::vector<int> scls, sseq;       // host: class and residue serial of each sorted point
+  void *arena = nullptr;
+  size_t bytes = 0;
+};
+
+// Device copy of a job.
+struct DevJobBuf {
+  DevJob dj{};                       // device pointers (host copy of the struct)
+  void *arena = nullptr;
+  size_t bytes = 0;
+  bool own_rec = false;
+  int pocket = 0;
+};
+
+int pocket_from_complex(const Complex *c, PocketData &pk);
+int job_from_complex(const Complex *c, int rep_begin, int rep_end, uint64_t seed, JobData &jd);
+int pocket_from_desc(const gd_pocket_desc_t &d, PocketData &pk);
+int job_from_desc(const gd_job_desc_t &d, int nprt, JobData &jd);
+
+// Replica layout of SetReplica (src/frontend/util.C:371-406).
+void default_replicas(int nlig, int nprt, int ntmp, std::vector<ReplicaMC> &out);
+
+void build_params(const EnePara &ep, const float move_scale[6], DevParams &p);
+
+int pack_pocket(const PocketData &pk, DevPocket &out);
+// rec: external device Record array (nullptr with want_records allocates one).
+int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
+             DevJobBuf &out);
+void free_pocket(DevPocket &p);
+void free_job(DevJobBuf &j);
+
+}  // namespace gd

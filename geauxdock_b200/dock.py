@@ -1,0 +1,156 @@
+"""Python mirror of the reference's GPU driver (src/main_gpu/geauxdock.C:285-339)
+over the drop-in C ABI: SetDevice, DeviceAlloc, InitCurand, then per complex
+SetParaT, CopyH2D, Dock; DeviceFree at the end.  Also thin wrappers of the
+additive entry points (pose evaluation, resident ensembles)."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import layout as Lo
+from ._lib import GD_PREC_FP32, check, load
+
+
+class ParaT(C.Structure):
+    _fields_ = [("rep_begin", C.c_int), ("rep_end", C.c_int), ("n_rep", C.c_int), ("record_sz", C.c_int)]
+
+
+class DockSession:
+    """Device buffers and RNG handles for `ngpu` GPUs, reused across complexes."""
+
+    def __init__(self, ngpu: int = 1, seed: int | None = None):
+        self.lib = load()
+        self.n = ngpu
+        check(self.lib.gd_set_ngpu(ngpu))
+        self.cd = (C.c_void_p * ngpu)()
+        self.rd = (C.c_void_p * ngpu)()
+        self.rng = (C.c_void_p * ngpu)()
+        self.parat = (ParaT * ngpu)()
+        self.pt = (C.POINTER(ParaT) * ngpu)(*[C.pointer(self.parat[g]) for g in range(ngpu)])
+        check(self.lib.SetDevice())
+        check(self.lib.DeviceAlloc(self.cd, self.rd, self.rng))
+        if seed is not None:
+            for g in range(ngpu):
+                check(self.lib.gd_rng_seed(self.rng[g], seed + g))
+        check(self.lib.InitCurand(self.rng))
+
+    def seed(self, seed: int) -> None:
+        for g in range(self.n):
+            check(self.lib.gd_rng_seed(self.rng[g], seed + g))
+
+    def dock(self, cx: np.ndarray, record: np.ndarray | None = None) -> np.ndarray:
+        """Dock one Complex record in place; returns the Record array (last dump chunk)."""
+        assert cx.dtype == Lo.COMPLEX
+        nrep = int(cx[0]["size"]["n_rep"])
+        if record is None:
+            record = Lo.aligned_zeros(Lo.RECORD, nrep)
+        ch = C.c_void_p(cx.ctypes.data)
+        check(self.lib.SetParaT(ch, self.pt))
+        check(self.lib.CopyH2D(ch, self.cd, self.pt))
+        check(self.lib.Dock(ch, C.c_void_p(record.ctypes.data), self.cd, self.rd, self.pt, self.rng))
+        return record
+
+    def close(self) -> None:
+        if self.cd is not None:
+            check(self.lib.DeviceFree(self.cd, self.rd, self.rng))
+            self.cd = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def eval_poses(cx: np.ndarray, conf: np.ndarray, mm: np.ndarray, precision: int = GD_PREC_FP32,
+               want64: bool = False):
+    """Energies of poses on the GPU: returns (out[n,10] float32, raw[n,9] float32, out64 or None)."""
+    lib = load()
+    conf = np.ascontiguousarray(conf, dtype=np.int32).reshape(-1, 2)
+    mm = np.ascontiguousarray(mm, dtype=np.float32).reshape(-1, 6)
+    n = len(conf)
+    out = np.zeros((n, 10), dtype=np.float32)
+    raw = np.zeros((n, 9), dtype=np.float32)
+    out64 = np.zeros((n, 10), dtype=np.float64) if want64 else None
+    check(lib.gd_eval_poses(C.c_void_p(cx.ctypes.data), n, C.c_void_p(conf.ctypes.data),
+                            C.c_void_p(mm.ctypes.data), precision, C.c_void_p(out.ctypes.data),
+                            C.c_void_p(out64.ctypes.data) if want64 else None, C.c_void_p(raw.ctypes.data)))
+    return out, raw, out64
+
+
+class Ensemble:
+    """A resident ensemble (gd_ensemble_*)."""
+
+    def __init__(self, handle: C.c_void_p, njob: int, keep=None):
+        self.lib = load()
+        self.h = handle
+        self.njob = njob
+        self._keep = keep
+
+    @classmethod
+    def from_complexes(cls, cxs, seeds, device: int = 0) -> "Ensemble":
+        lib = load()
+        arr = (C.c_void_p * len(cxs))(*[c.ctypes.data for c in cxs])
+        sd = (C.c_uint64 * len(cxs))(*seeds)
+        h = C.c_void_p()
+        check(lib.gd_ensemble_create_complex(arr, len(cxs), sd, device, C.byref(h)))
+        return cls(h, len(cxs))
+
+    @classmethod
+    def from_jobs(cls, pockets, jobs, enepara: np.ndarray, device: int = 0) -> "Ensemble":
+        from . import synth
+
+        lib = load()
+        keep: list = []
+        from ._lib import JobDesc, PocketDesc
+
+        parr = (PocketDesc * len(pockets))(*[synth.pocket_desc(p, keep) for p in pockets])
+        jarr = (JobDesc * len(jobs))(*[synth.job_desc(j, keep) for j in jobs])
+        ep = np.array([enepara], dtype=Lo.ENEPARA)
+        keep.append(ep)
+        h = C.c_void_p()
+        check(lib.gd_ensemble_create(parr, len(pockets), jarr, len(jobs), C.c_void_p(ep.ctypes.data), device,
+                                     C.byref(h)))
+        return cls(h, len(jobs), keep)
+
+    def init(self) -> None:
+        check(self.lib.gd_ensemble_init(self.h))
+
+    def run(self, nsteps: int, steps_per_exchange: int = 0) -> None:
+        check(self.lib.gd_ensemble_run(self.h, nsteps, steps_per_exchange))
+
+    def sync(self):
+        ms = C.c_double()
+        nl = C.c_int()
+        check(self.lib.gd_ensemble_sync(self.h, C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value
+
+    def replicas(self, job: int = 0) -> np.ndarray:
+        n = check(self.lib.gd_ensemble_num_replicas(self.h, job))
+        out = Lo.aligned_zeros(Lo.REPLICA, n)
+        check(self.lib.gd_ensemble_replicas(self.h, job, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def stats(self, job: int = 0) -> np.ndarray:
+        n = check(self.lib.gd_ensemble_num_replicas(self.h, job))
+        out = np.zeros((n, 8), dtype=np.float64)
+        check(self.lib.gd_ensemble_stats(self.h, job, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def autotune(self, steps: int = 4) -> str:
+        buf = C.create_string_buffer(8192)
+        check(self.lib.gd_ensemble_autotune(self.h, steps, buf, len(buf)))
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.gd_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,173 @@
+/*
+ * gdock.h -- C ABI of libgdock.so, the B200 (sm_100a) Monte Carlo docking
+ * backend.
+ *
+ * Part 1 is the drop-in boundary: the functions a GeauxDock frontend calls
+ * around its GPU backend, with the reference's names and argument shapes.
+ * Two deliberate changes from the reference signatures:
+ *   - every function returns int (GD_OK = 0, negative GD_E_* on failure;
+ *     gd_last_error() gives the message) where the reference prints and
+ *     calls exit() (src/module/yeah/cuda/runtime/wrapper.h:21-64);
+ *   - curandState** becomes gd_rng_t**, an opaque counter-based Philox
+ *     handle (seeded, reproducible) in place of time-seeded XORWOW states
+ *     (src/backend_gpu/backend_gpu.cu:49-59).
+ * The array arguments (Complex **cd, Record **rd, ParaT **pt, gd_rng_t **rng)
+ * have one entry per GPU, as the reference's cd[NGPU] arrays
+ * (src/main_gpu/geauxdock.C:296-302); the GPU count is gd_set_ngpu()
+ * (default 1, or the GDOCK_NGPU environment variable).
+ *
+ * Part 2 is additive: pose evaluation, resident batched ensembles, and the
+ * serving loop.  All sizes are plain ints, all data plain pointers.
+ */
+#ifndef GDOCK_H
+#define GDOCK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "gdock_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define GD_OK 0
+#define GD_E_INVALID (-1)   /* malformed input (types, sizes, indices)           */
+#define GD_E_NOMEM (-2)     /* device or host allocation failed                  */
+#define GD_E_CAPACITY (-3)  /* input exceeds a capacity limit                    */
+#define GD_E_CUDA (-4)      /* CUDA runtime error                                */
+#define GD_E_TIMEOUT (-5)   /* a bounded device wait gave up                     */
+#define GD_E_NODEVICE (-6)  /* no usable GPU                                     */
+#define GD_E_STATE (-7)     /* call out of order (e.g. Dock before DeviceAlloc)  */
+#define GD_E_BUSY (-8)      /* serving loop: admission refused (budget, queue)   */
+#define GD_E_CANCELLED (-9) /* serving loop: request cancelled                   */
+
+/* Message of the last failure on the calling thread. */
+const char *gd_last_error(void);
+
+/* Number of GPUs the reference-boundary functions spread replicas over. */
+int gd_set_ngpu(int n);
+int gd_get_ngpu(void);
+
+/* ================================================ Part 1: drop-in boundary */
+
+typedef struct gd_rng gd_rng_t;
+
+/* src/backend_gpu/prepair.h:4 -- select the devices (prefers shared memory). */
+int SetDevice(void);
+/* src/backend_gpu/prepair.h:5 -- per GPU: device Complex, Record[GD_MAX_REP], RNG handle. */
+int DeviceAlloc(Complex **cd, Record **rd, gd_rng_t **rng);
+/* src/backend_gpu/prepair.h:6 */
+int DeviceFree(Complex **cd, Record **rd, gd_rng_t **rng);
+/* src/backend_gpu/prepair.h:7 -- contiguous replica range per GPU (prepair.C:64-115);
+ * with replica exchange on, ranges are cut at protein-conformation boundaries. */
+int SetParaT(Complex *ch, ParaT **pt);
+/* src/backend_gpu/prepair.h:8 -- ch->rep_begin/rep_end set per GPU, Complex copied. */
+int CopyH2D(Complex *ch, Complex **cd, ParaT **pt);
+/* src/backend_gpu/backend_gpu.h:4 -- seed the Philox handles (time-seeded like the
+ * reference unless gd_rng_seed() or GDOCK_SEED fixed the seed). */
+int InitCurand(gd_rng_t **rng);
+/* Fix the seed of one handle (reproducible runs); resets its call counter. */
+int gd_rng_seed(gd_rng_t *rng, uint64_t seed);
+/* src/backend_gpu/backend_gpu.h:6-11 -- initial energy (forced accept), then
+ * steps_total MC steps in chunks of steps_per_dump; after each chunk the
+ * replicas' Record entries are copied to rh[rep_begin..rep_end].  Final
+ * replica states are left in cd[g]->replica[] and also copied to
+ * ch->replica[].  mcpara.steps_per_exchange > 0 adds a replica-exchange sweep
+ * every that many steps (new; the reference parses but never runs it). */
+int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_t **rng);
+
+/* ============================================================ Part 2: additive */
+
+/* Kernel and precision used by Dock and the ensembles. */
+#define GD_KERNEL_BATCHED 0   /* one warp per replica, persistent, staged pocket */
+#define GD_KERNEL_PLAIN 1     /* one CTA per replica, the reference's structure   */
+#define GD_PREC_FP32 0        /* FP32 pair energies, plain reductions             */
+#define GD_PREC_FP32_KAHAN 1  /* FP32 pair energies, compensated reductions       */
+#define GD_PREC_FP64 2        /* FP64 pair energies                               */
+
+/* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*), "warps" (replicas
+ * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape).  Applies to objects
+ * created afterwards on the calling process. */
+int gd_set_option(const char *name, long long value);
+long long gd_get_option(const char *name);
+
+/* Energies of n poses of Complex c: pose i is ligand conformation conf[2i],
+ * protein conformation conf[2i+1], movematrix mm[6i..6i+5].  out[10i..]:
+ * the ten ReplicaMC.energy terms; raw[9i..] (may be NULL): the terms before
+ * the per-atom division and normalisation; out64 (may be NULL): FP64 copy of
+ * out (exact only with GD_PREC_FP64).  Host buffers; runs on GPU 0. */
+int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int precision, float *out,
+                  double *out64, float *raw);
+
+/* OptimizeEnepara (src/frontend/util_optimize_soa.C:489-540): raw parameters
+ * -> the precomputed tables of EnePara, bit-identical to the reference. */
+int gd_optimize_enepara(const EnePara0 *in, EnePara *out);
+
+/* Cap-free description of one docking job (ligand sizes above GD_MAXLIG and
+ * pockets above GD_MAXPRO are allowed).  Arrays are dense, C order. */
+typedef struct gd_job_desc {
+  int natom, nlig;            /* ligand atoms, ligand conformations           */
+  const float *lig_xyz;       /* [nlig][natom][3] in the ligand-centre frame  */
+  const int *lig_type;        /* [natom] 0..23                                */
+  const float *lig_charge;    /* [natom]                                      */
+  const float *lig_center;    /* [nlig][3] lab frame                          */
+  int pocket;                 /* index of a pocket from gd_pocket_desc_t list */
+  int nkde;
+  const float *kde_xyz;       /* [nkde][3]                                    */
+  const int *kde_type;        /* [nkde]                                       */
+  int nmcs;
+  const float *mcs_xyz;       /* [nmcs][natom][3], GD_MCS_INVALID_COORD = unset */
+  const float *mcs_tcc;       /* [nmcs]                                       */
+  int psp_ncol;               /* columns of psp (residue serial numbers)      */
+  const float *psp;           /* [24][psp_ncol] pocket-specific potential     */
+  int ntmp;
+  const float *temperature;   /* [ntmp] temperatures T (minus_beta = -1/T)    */
+  float move_scale[6];
+  uint64_t seed;
+} gd_job_desc_t;
+
+typedef struct gd_pocket_desc {
+  int npoint, nconf;
+  const float *xyz;           /* [nconf][npoint][3]                           */
+  const int *type;            /* [npoint] point type 0..29                    */
+  const int *cls;             /* [npoint] point class c (0..3)                */
+  const int *cdc;             /* [npoint] hydrophobic-contact flag            */
+  const int *seq3r;           /* [npoint] residue serial number (psp column)  */
+  const float *hpp;           /* [npoint]                                     */
+  const float *ele;           /* [npoint]                                     */
+  const float *center;        /* [nconf][3] pocket centre                     */
+} gd_pocket_desc_t;
+
+/* A resident ensemble: many jobs, their pockets, replica states and FP64
+ * statistics kept in device memory and advanced by one persistent launch
+ * per chunk (captured in a CUDA graph).  Replica r of job j is ligand conf
+ * l, protein conf p, temperature t with r = ntmp*nlig*p + nlig*t + l. */
+typedef struct gd_ensemble gd_ensemble_t;
+
+int gd_ensemble_create(const gd_pocket_desc_t *pockets, int npocket, const gd_job_desc_t *jobs, int njob,
+                       const EnePara *enepara, int device, gd_ensemble_t **out);
+/* The same from reference-layout Complexes (one job each; identical proteins share a pocket). */
+int gd_ensemble_create_complex(const Complex *const *cx, int n, const uint64_t *seeds, int device,
+                               gd_ensemble_t **out);
+/* Initial energies (no move, forced accept). */
+int gd_ensemble_init(gd_ensemble_t *e);
+/* Advance every replica by nsteps MC steps, with a replica-exchange sweep
+ * every steps_per_exchange steps (0 = none).  Asynchronous. */
+int gd_ensemble_run(gd_ensemble_t *e, int nsteps, int steps_per_exchange);
+/* Wait for the device; kernel_ms: device time of the MC kernels since the
+ * last call (CUDA events on the ensemble's stream), launches: their count. */
+int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches);
+int gd_ensemble_num_replicas(const gd_ensemble_t *e, int job);
+int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out);
+/* Per replica: {n_steps, n_accept, n_exch_try, n_exch_acc, mean E, var E, best E, best step}. */
+int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8);
+/* Choose the tile shape by timing candidates on a snapshot (state restored). */
+int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len);
+int gd_ensemble_destroy(gd_ensemble_t *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GDOCK_H */

@@ -1,0 +1,110 @@
+"""ctypes access to the checkers (TEST INFRASTRUCTURE ONLY).
+
+liboracle.so  -- the FP64 C restatement (gd_oracle.c).
+_ref/libgdref.so -- the reference's own CPU code built from its sources.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+these; the product never does.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libgdref.so"
+
+_ora = None
+_ref = None
+
+
+def build(reference: str | None = None) -> None:
+    """make the FP64 oracle (always) and the reference library (when the sources are present)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    ref = reference or os.environ.get("GD_REFERENCE", "/root/reference")
+    if Path(ref, "src").is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
+
+
+def oracle() -> C.CDLL:
+    global _ora
+    if _ora is None:
+        lib = C.CDLL(str(ORACLE_SO))
+        vp = C.c_void_p
+        lib.gdo_energy.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp]
+        lib.gdo_montecarlo.argtypes = [vp, vp, C.c_int, C.c_int, C.c_uint64, C.c_int]
+        lib.gdo_exchange.argtypes = [vp, C.c_int, C.c_uint64]
+        lib.gdo_philox4x32_10.argtypes = [vp, vp, vp]
+        lib.gdo_u01.argtypes = [C.c_uint32]
+        lib.gdo_u01.restype = C.c_float
+        _ora = lib
+    return _ora
+
+
+def have_ref() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(str(REF_SO))
+        vp = C.c_void_p
+        lib.gdref_dock.argtypes = [vp, vp]
+        lib.gdref_montecarlo.argtypes = [vp, vp, C.c_int, C.c_int]
+        lib.gdref_set_threads.argtypes = [C.c_int]
+        lib.gdref_max_threads.restype = C.c_int
+        lib.gdref_sizeof.argtypes = [C.c_char_p]
+        lib.gdref_sizeof.restype = C.c_size_t
+        lib.gdref_load_enepara.argtypes = [C.c_char_p] * 4 + [vp, vp]
+        lib.gdref_load_complex.argtypes = [C.c_char_p] * 8 + [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                                               C.c_int, C.c_int, vp]
+        _ref = lib
+    return _ref
+
+
+def energy(cx: np.ndarray, il: int, ip: int, mm) -> tuple[np.ndarray, np.ndarray]:
+    """FP64 oracle energy of one pose: (e[10], raw[9])."""
+    m = np.ascontiguousarray(mm, dtype=np.float32)
+    e = np.zeros(10)
+    raw = np.zeros(9)
+    oracle().gdo_energy(cx.ctypes.data, il, ip, m.ctypes.data, e.ctypes.data, raw.ctypes.data)
+    return e, raw
+
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    o = np.zeros(4, dtype=np.uint32)
+    oracle().gdo_philox4x32_10(c.ctypes.data, k.ctypes.data, o.ctypes.data)
+    return o
+
+
+def montecarlo(cx: np.ndarray, record, s1: int, s2max: int, seed: int, steps_per_exchange: int = 0) -> None:
+    oracle().gdo_montecarlo(cx.ctypes.data, None if record is None else record.ctypes.data, s1, s2max, seed,
+                            steps_per_exchange)
+
+
+def ref_energies(cx: np.ndarray, reps: np.ndarray | None = None) -> np.ndarray:
+    """The reference's own FP32 energy of every replica's stored pose: MonteCarlo_d with
+    s2max == 1 (no move, forced accept; kernel_cpp_montecarlo_soa.C:248, :384).  Returns
+    energy[n_rep, 10]; cx is not modified."""
+    from geauxdock_b200 import layout as Lo
+
+    work = cx.copy()
+    if reps is not None:
+        work[0]["replica"][: len(reps)] = reps
+    n = int(work[0]["size"]["n_rep"])
+    work[0]["rep_begin"], work[0]["rep_end"] = 0, n - 1
+    for r in range(n):
+        work[0]["replica"][r]["is_accept"] = 0
+    rec = Lo.aligned_zeros(Lo.RECORD, n)
+    ref().gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, 1)
+    return np.array(work[0]["replica"]["energy"][:n])
