@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""MC pose-evals/s of the B200 docking backend on the replica-ensemble workload.
+
+Workload (one rank = one GPU): one synthetic complex with a 40-atom ligand in
+20 conformations, 11 protein conformations of 1500 points, 400 KDE points,
+16 MCS templates and 16 temperatures 0.3..3.0 -- 3520 replicas -- with a
+replica-exchange sweep every 50 MC steps.  One bench step = one exchange
+interval: 50 MC steps of all 3520 replicas plus the exchange sweep.
+
+value      pose-evals/s over all ranks, device time (CUDA events on the
+           library's stream), inputs resident in HBM, L2 flushed between steps
+e2e        the same metric through the drop-in C ABI with host buffers
+           (SetParaT + CopyH2D + Dock of steps_total = 200, Record copies back)
+roofline   the batched Monte Carlo kernel against the measured FP32 FMA peak
+plain      the plain kernel (the reference's launch structure) on the same work
+cpu_baseline  the reference's own CPU Monte Carlo (built from its sources) on
+           the box's host cores, a bounded sample of the same workload
+
+--impl reference runs the reference's CPU implementation instead (rank 0).
+Multi-GPU (torchrun): each rank runs its own ensemble (weak scaling, no
+data-path collective); timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MC pose-evals/s batched+served vs plain kernel on 1 B200; p50/p99 dock latency"
+UNIT = "pose-evals/s"
+STEPS_PER_INTERVAL = 50
+
+
+def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous shard [b, e) of n units for rank (the reference's maximising-balance split)."""
+    per = -(-n // world)
+    b = min(per * rank, n)
+    return b, min(b + per, n)
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait(timeout=10)
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        load = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _workload(rank: int):
+    from geauxdock_b200 import params, synth
+
+    ep = params.optimize_enepara(params.default_enepara0())
+    pk, job = synth.config2(seed=1 + rank)
+    return ep, pk, job
+
+
+def _config(n_rep: int, world: int, extra: dict | None = None) -> dict:
+    c = {"workload": "replica ensemble: 1 complex, ligand 40 atoms x 20 conformations, pocket 1500 points x 11 "
+                     "conformations, 400 KDE points, 16 MCS templates, 16 temperatures 0.3-3.0, exchange every "
+                     f"{STEPS_PER_INTERVAL} steps",
+         "replicas_per_gpu": n_rep, "mc_steps_per_bench_step": STEPS_PER_INTERVAL,
+         "parallelism": f"replica shards x{world} (independent ensembles per GPU)",
+         "l2": "flushed between timed steps (256 MiB write)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def cpu_reference_sample(cx, seconds: float) -> dict:
+    """The reference's own CPU Monte Carlo (MonteCarlo_d, OpenMP over replicas) on
+    all replicas of the complex for a number of steps sized to ~`seconds`."""
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    from geauxdock_b200 import layout as Lo
+    from oracle import oracle as O
+
+    if not O.have_ref():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libgdref.so was not built (reference sources absent)"}
+    ref = O.ref()
+    cores = os.cpu_count() or 1
+    ref.gdref_set_threads(cores)
+    work = cx.copy()
+    n = int(work[0]["size"]["n_rep"])
+    rec = Lo.aligned_zeros(Lo.RECORD, n)
+    ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, 1)     # initial energies
+    t0 = time.perf_counter()
+    ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, 2)     # calibration: 2 steps
+    t2 = time.perf_counter() - t0
+    steps = int(max(2, min(200, round(seconds / max(t2 / 2, 1e-6)))))
+    t0 = time.perf_counter()
+    ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 2, steps)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{n} replicas x {steps} MC steps of the same complex, reference MonteCarlo_d "
+                      f"(g++ -O3 -fopenmp, OMP_NUM_THREADS={cores}), {dt:.1f} s"}
+
+
+def run_reference(args) -> None:
+    rank, world, local = _dist()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    from geauxdock_b200 import layout as Lo, synth
+    from oracle import oracle as O
+
+    ep, pk, job = _workload(0)
+    cx = synth.to_complex(job, pk, ep, steps_per_exchange=STEPS_PER_INTERVAL)
+    n = int(cx[0]["size"]["n_rep"])
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgdref.so not built: the reference "
+                                                              "sources were absent when build() ran"}))
+        return
+    ref = O.ref()
+    cores = os.cpu_count() or 1
+    ref.gdref_set_threads(cores)
+    rec = Lo.aligned_zeros(Lo.RECORD, n)
+    ref.gdref_montecarlo(cx.ctypes.data, rec.ctypes.data, 0, 1)
+    per_step = 2            # MC steps of all replicas per bench step (a bounded sample)
+    s = 0
+    for _ in range(args.warmup):
+        ref.gdref_montecarlo(cx.ctypes.data, rec.ctypes.data, s, per_step)
+        s += per_step
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.gdref_montecarlo(cx.ctypes.data, rec.ctypes.data, s, per_step)
+        s += per_step
+    dt = time.perf_counter() - t0
+    value = n * per_step * args.steps / dt
+    sample = (f"{n} replicas x {per_step} MC steps per bench step, reference MonteCarlo_d built from its sources "
+              f"(g++ -O3 -fopenmp, OMP_NUM_THREADS={cores})")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, Astex-like shapes)",
+        "config": _config(n, 1, {"sample": sample}), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_ours(args) -> None:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from geauxdock_b200 import dock, layout as Lo, synth, workmodel
+    from geauxdock_b200._lib import check, load
+
+    lib = load()
+    ep, pk, job = _workload(rank)
+    cx = synth.to_complex(job, pk, ep, steps_total=200, steps_per_dump=200, steps_per_exchange=STEPS_PER_INTERVAL)
+    n_rep = int(cx[0]["size"]["n_rep"])
+    fpp = workmodel.job_flops_per_pose(job, pk, ep)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- resident ensemble, batched kernel
+    check(lib.gd_set_option(b"kernel", 0))
+    ens = dock.Ensemble.from_complexes([cx], [1000 + rank], device=local)
+    ens.init()
+    ens.sync()
+    tune = "" if args.no_autotune else ens.autotune(4)
+    stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        ens.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+    ens.sync()
+    barrier()
+    clocks = Clocks(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            ens.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+            flush.zero_()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    kernel_ms, mc_launches = ens.sync()
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    pose_evals = n_rep * STEPS_PER_INTERVAL * args.steps
+    value = world * pose_evals / (ms_max / 1e3)
+    avg_launch_ms = kernel_ms / max(mc_launches, 1)
+    flops_per_launch = fpp * n_rep * STEPS_PER_INTERVAL
+    peak = C.c_double()
+    check(lib.gd_fp32_peak(C.byref(peak)))
+    achieved = flops_per_launch / (avg_launch_ms / 1e3) / 1e12
+    ens.close()
+
+    # ---------------- plain kernel, same work
+    check(lib.gd_set_option(b"kernel", 1))
+    plain = dock.Ensemble.from_complexes([cx], [1000 + rank], device=local)
+    plain.init()
+    plain.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+    plain.sync()
+    p_steps = 2
+    pstream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(plain.h), device=torch.device("cuda", local))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(pstream)
+    for _ in range(p_steps):
+        plain.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+    b.record(pstream)
+    b.synchronize()
+    plain_value = n_rep * STEPS_PER_INTERVAL * p_steps / (a.elapsed_time(b) / 1e3)
+    plain.close()
+    check(lib.gd_set_option(b"kernel", 0))
+
+    # ---------------- end to end through the drop-in C ABI, pinned host buffers
+    cx_pin = torch.empty(Lo.COMPLEX.itemsize, dtype=torch.uint8, pin_memory=True)
+    cx_h = np.frombuffer(cx_pin.numpy(), dtype=Lo.COMPLEX, count=1)
+    cx_h[0] = cx[0]
+    rec_pin = torch.empty(Lo.RECORD.itemsize * n_rep, dtype=torch.uint8, pin_memory=True)
+    rec_h = np.frombuffer(rec_pin.numpy(), dtype=Lo.RECORD, count=n_rep)
+    with dock.DockSession(1, seed=77 + rank) as s:
+        s.dock(cx_h, rec_h)              # warm-up (also the first-use cost of the library)
+        cx_h[0] = cx[0]
+        barrier()
+        t0 = time.perf_counter()
+        s.dock(cx_h, rec_h)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    e2e_steps = int(cx[0]["mcpara"]["steps_total"])
+    e2e_value = world * n_rep * e2e_steps / e2e_s
+
+    if rank == 0:
+        cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "skipped (--no-cpu-baseline)"}
+        if not args.no_cpu_baseline and world == 1:
+            cpu = cpu_reference_sample(cx, args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, Astex-like shapes)",
+            "config": _config(n_rep, world, {"autotune": tune.strip().splitlines()[-1] if tune else "off"}),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": Lo.COMPLEX.itemsize,
+                    "d2h_bytes_per_step": Lo.RECORD.itemsize * n_rep + Lo.REPLICA.itemsize * n_rep,
+                    "step": f"one Dock call: CopyH2D + initial energies + {e2e_steps} MC steps + Record copy"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value, "traffic": None,
+                         "kernel": "gd::mc_kernel (batched Monte Carlo, 50 steps x 3520 replicas per launch)",
+                         "flops_per_pose_eval": fpp, "avg_launch_ms": avg_launch_ms,
+                         "peak_source": "measured this run: FP32 FMA microbenchmark gd_fp32_peak (2 flops/FMA); "
+                                        "MEASURED_PEAKS.json has no FP32 figure"},
+            "plain_kernel": {"value": plain_value, "unit": UNIT, "speedup_batched_over_plain": value / world / plain_value},
+            "cpu_baseline": cpu,
+            "clocks": ck,
+            "gpu_launches": 2 * args.steps,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

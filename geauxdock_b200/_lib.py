@@ -39,7 +39,7 @@ EXPORTED = [
     "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy",
-    "gd_layout", "gd_optimize_enepara",
+    "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
 ]
 
 
@@ -102,6 +102,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_stats": (i, [vp, i, vp]), "gd_ensemble_autotune": (i, [vp, i, C.c_char_p, i]),
         "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),
         "gd_optimize_enepara": (i, [vp, vp]),
+        "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

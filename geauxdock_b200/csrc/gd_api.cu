@@ -1050,3 +1050,53 @@ extern "C" int gd_optimize_enepara(const EnePara0 *e0, EnePara *e)
   }
   return GD_OK;
 }
+
+// ------------------------------------------------------------ timing --
+extern "C" void *gd_ensemble_stream(const gd_ensemble_t *e) { return e ? (void *)e->st : nullptr; }
+
+namespace {
+// Independent FMA chains: 8 accumulators per thread so the FMA pipe, not
+// latency, bounds the loop; the result is stored so nothing is dead code.
+__global__ void fma_peak_kernel(float *out, int iters, float a, float b)
+{
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+        x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+}  // namespace
+
+// Measured FP32 FMA throughput of the current device in TFLOP/s (2 flops per FMA).
+extern "C" int gd_fp32_peak(double *tflops)
+{
+  if (!tflops) return fail(GD_E_INVALID, "null argument");
+  int dev = 0, nsm = 0;
+  GD_CUDA(cudaGetDevice(&dev));
+  GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int threads = 512, blocks = nsm * 4, iters = 4096;
+  float *out = nullptr;
+  GD_CUDA(cudaMalloc(&out, sizeof(float) * threads * blocks));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fma_peak_kernel<<<blocks, threads>>>(out, 64, 0.999f, 1e-3f);  // warm-up
+  cudaEventRecord(a);
+  fma_peak_kernel<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
+  cudaEventRecord(b);
+  const cudaError_t e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (e != cudaSuccess) return fail(GD_E_CUDA, "gd_fp32_peak: %s", cudaGetErrorString(e));
+  const double flops = 2.0 * 8.0 * 16.0 * (double)iters * threads * blocks;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return GD_OK;
+}

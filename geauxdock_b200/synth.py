@@ -46,6 +46,7 @@ class Pocket:
     ele: np.ndarray          # [P]
     center: np.ndarray       # [nconf, 3]
     nres: int
+    res: np.ndarray = None   # [P] residue code of each point
 
     @property
     def npoint(self) -> int:
@@ -134,7 +135,7 @@ def make_pocket(rng: np.random.Generator, npoint: int, nconf: int, ep0=None, cen
     hpp = ep0["hpp"][d].astype(np.float32)
     ele = np.where(t == 0, ep0["ele"][d + 30], ep0["ele"][t]).astype(np.float32)
     centers = np.tile(cen.astype(np.float32), (nconf, 1))
-    return Pocket(xyz, t, c, cdc, seq, hpp, ele, centers, k)
+    return Pocket(xyz, t, c, cdc, seq, hpp, ele, centers, k, d)
 
 
 def _chain(rng: np.random.Generator, L: int) -> np.ndarray:

@@ -166,6 +166,12 @@ int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8);
 /* Choose the tile shape by timing candidates on a snapshot (state restored). */
 int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len);
 int gd_ensemble_destroy(gd_ensemble_t *e);
+/* The CUDA stream (cudaStream_t) the ensemble launches on, for event timing. */
+void *gd_ensemble_stream(const gd_ensemble_t *e);
+
+/* Measured FP32 FMA throughput of the current GPU (TFLOP/s, 2 flops per FMA):
+ * the denominator of the pair kernel's roofline. */
+int gd_fp32_peak(double *tflops);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,128 @@
+"""GPU pose energies (gd_eval_poses, the batched kernel's energy code) against
+the FP64 oracle and the reference's own FP32 routine, per term.
+
+Tolerance: the ten ReplicaMC.energy terms are normalised (a_i * E_i / L + b_i)
+to unit scale, so each GPU term must satisfy
+    |e_gpu - e_64| <= tol * max(|e_64|, 1)
+with tol = 1e-5 for the FP32 kernels and 1e-9 for the FP64 kernel (compared
+in FP64).  Against the reference's own FP32 routine the bound is REF_TOL, the
+reference's own distance from FP64.
+"""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from geauxdock_b200 import dock, synth
+from geauxdock_b200._lib import GD_PREC_FP32, GD_PREC_FP32_KAHAN, GD_PREC_FP64
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL32 = 1e-5
+TOL64 = 1e-9
+REF_TOL = 5e-5   # the reference's own FP32 routine vs FP64 (tests/test_oracle.py)
+
+
+def _oracle_energies(O, cx, conf, mm):
+    return np.array([O.energy(cx, int(c[0]), int(c[1]), m)[0] for c, m in zip(conf, mm)])
+
+
+def _check(e, ref, tol, what):
+    err = np.abs(np.asarray(e, np.float64) - ref) / np.maximum(np.abs(ref), 1.0)
+    worst = np.unravel_index(np.argmax(err), err.shape)
+    assert err.max() <= tol, f"{what}: max scaled error {err.max():.3g} at pose {worst[0]} term {worst[1]}"
+    return err.max(axis=0)
+
+
+@pytest.mark.parametrize("prec,tol", [(GD_PREC_FP32, TOL32), (GD_PREC_FP32_KAHAN, TOL32), (GD_PREC_FP64, TOL32)])
+def test_golden_config1(lib, enepara, prec, tol):
+    """Committed poses of config 1 against the committed reference FP32 and FP64 energies."""
+    g = np.load(GOLDEN / "ref_energies_c1.npz")
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara)
+    conf = np.zeros((len(g["mm"]), 2), np.int32)
+    out, raw, _ = dock.eval_poses(cx, conf, g["mm"], prec)
+    _check(out, g["e64"], tol, "vs FP64 oracle")
+    _check(out, g["e_ref"].astype(np.float64), REF_TOL, "vs reference FP32")
+
+
+def test_fp64_kernel_matches_oracle(lib, enepara, oracle_lib):
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara)
+    mm = synth.config4_poses(21, 48, radius=5.0)
+    conf = np.zeros((48, 2), np.int32)
+    _, _, out64 = dock.eval_poses(cx, conf, mm, GD_PREC_FP64, want64=True)
+    ref = _oracle_energies(oracle_lib, cx, conf, mm)
+    # FP64 pair arithmetic; the float constants -1/sqrt(2 pi) and 1/kde3 of the
+    # reference (kernel_cuda_l1_montecarlo.cu:14, :194) bound terms 4 and 6 at ~1e-7
+    err = np.abs(out64 - ref) / np.maximum(np.abs(ref), 1.0)
+    assert np.delete(err, [4, 6, 9], axis=1).max() <= TOL64
+    assert err.max() <= 2e-7
+
+
+@pytest.mark.parametrize("prec", [GD_PREC_FP32, GD_PREC_FP32_KAHAN])
+def test_ensemble_all_conformations(lib, enepara, oracle_lib, prec):
+    """Every (ligand conf, protein conf) pair of a multi-conformation complex,
+    poses spread over the pocket, against the oracle."""
+    rng = np.random.default_rng(12)
+    pk = synth.make_pocket(rng, 1100, 4)
+    job = synth.make_job(rng, pk, 47, 5, 350, 11, [1.0], seed=2)
+    cx = synth.to_complex(job, pk, enepara)
+    conf = np.array([(l, p) for l in range(5) for p in range(4)] * 3, np.int32)
+    mm = synth.config4_poses(13, len(conf), radius=6.0)
+    out, raw, _ = dock.eval_poses(cx, conf, mm, prec)
+    _check(out, _oracle_energies(oracle_lib, cx, conf, mm), TOL32, "ensemble vs oracle")
+
+
+def test_edge_sizes(lib, enepara, oracle_lib):
+    """Tiny and cap-sized complexes: 1 atom / 1 point / no KDE points of the ligand's
+    types; 64 atoms x 2048 points (the reference's MAXLIG x MAXPRO)."""
+    rng = np.random.default_rng(3)
+    for L, P, K, M in [(1, 1, 0, 1), (2, 5, 3, 1), (64, 2048, 1000, 32), (31, 129, 40, 3)]:
+        pk = synth.make_pocket(rng, P, 1)
+        job = synth.make_job(rng, pk, L, 1, K, M, [1.0], seed=1)
+        cx = synth.to_complex(job, pk, enepara)
+        mm = synth.config4_poses(L + P, 12, radius=5.0)
+        conf = np.zeros((12, 2), np.int32)
+        out, _, _ = dock.eval_poses(cx, conf, mm, GD_PREC_FP32)
+        _check(out, _oracle_energies(oracle_lib, cx, conf, mm), TOL32, f"L={L} P={P}")
+
+
+def test_reference_fp32_direct(lib, enepara, oracle_lib):
+    """GPU against the reference's own CPU energy routine run here (oracle/_ref),
+    on config 2 (40 atoms x 1500 points): the GPU is within 1e-5 of FP64, and
+    within the reference's own distance from FP64 (+1e-5) of the reference."""
+    if not oracle_lib.have_ref():
+        pytest.skip("reference library not built")
+    pk, job = synth.config2(1)
+    cx = synth.to_complex(job, pk, enepara)
+    n = 64
+    mm = synth.config4_poses(31, n, radius=5.0)
+    work = cx.copy()
+    conf = np.zeros((n, 2), np.int32)
+    for i in range(n):
+        r = work[0]["replica"][i * 50]
+        r["movematrix"] = mm[i]
+        conf[i] = (r["idx_lig"], r["idx_prt"])
+    e_ref = oracle_lib.ref_energies(work)[np.arange(n) * 50].astype(np.float64)
+    e64 = _oracle_energies(oracle_lib, cx, conf, mm)
+    out, _, _ = dock.eval_poses(cx, conf, mm, GD_PREC_FP32)
+    _check(out, e64, TOL32, "vs FP64 oracle")
+    scale = np.maximum(np.abs(e64), 1.0)
+    ref_err = np.abs(e_ref - e64) / scale
+    gap = np.abs(out.astype(np.float64) - e_ref) / scale
+    assert np.all(gap <= ref_err + TOL32), float((gap - ref_err).max())
+
+
+def test_eval_order_independent(lib, enepara):
+    """Results do not depend on how poses are grouped into CTAs."""
+    pk, job = synth.config2(1)
+    cx = synth.to_complex(job, pk, enepara)
+    rng = np.random.default_rng(0)
+    conf = np.stack([rng.integers(0, 20, 100), rng.integers(0, 11, 100)], axis=1).astype(np.int32)
+    mm = synth.config4_poses(2, 100)
+    a, _, _ = dock.eval_poses(cx, conf, mm)
+    perm = rng.permutation(100)
+    b, _, _ = dock.eval_poses(cx, conf[perm], mm[perm])
+    np.testing.assert_array_equal(a[perm], b)

@@ -1,0 +1,183 @@
+"""GPU Monte Carlo against the FP64 oracle driven by the same Philox draws:
+trajectories, Record contents of the drop-in Dock path, replica exchange, the
+plain kernel, reproducibility and tile-shape independence."""
+
+import numpy as np
+import pytest
+
+from geauxdock_b200 import dock, layout as Lo, synth
+from geauxdock_b200._lib import GD_E_INVALID, GdockError, check
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_ensemble(enepara, seed=4, L=18, P=300, nlig=3, nprt=2, temps=(0.3, 0.6, 1.2, 2.4)):
+    rng = np.random.default_rng(seed)
+    pk = synth.make_pocket(rng, P, nprt)
+    job = synth.make_job(rng, pk, L, nlig, 120, 6, np.array(temps, np.float32), seed=seed)
+    return synth.to_complex(job, pk, enepara)
+
+
+def _oracle_run(O, cx, seed, steps, spx=0, record=None):
+    ref = cx.copy()
+    O.montecarlo(ref, record, 0, 1, seed)
+    if steps:
+        O.montecarlo(ref, record, 0, steps, seed, spx)
+    return ref
+
+
+def _close(a, b, tol=1e-5):
+    """Energies agree to tol in the terms' normalised scale: |a - b| <= tol * max(|b|, 1)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    assert np.all(np.abs(a - b) <= tol * np.maximum(np.abs(b), 1.0)), float(
+        (np.abs(a - b) / np.maximum(np.abs(b), 1.0)).max())
+
+
+def _same_trajectory(got, want):
+    """Replicas whose final pose matches the oracle exactly (the same accepted moves)."""
+    return np.all(got["movematrix"] == want["movematrix"], axis=1)
+
+
+def test_single_replica_trajectory(lib, enepara, oracle_lib):
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara)
+    ref = _oracle_run(oracle_lib, cx, 7, 300)
+    with dock.Ensemble.from_complexes([cx], [7]) as ens:
+        ens.init()
+        ens.run(300)
+        ens.sync()
+        got = ens.replicas(0)
+        st = ens.stats(0)
+    want = ref[0]["replica"][:1]
+    assert _same_trajectory(got, want).all()
+    _close(got["energy"], want["energy"])
+    assert st[0, 0] == 301 and 0 < st[0, 1] <= 301
+
+
+def test_ensemble_with_exchange(lib, enepara, oracle_lib):
+    cx = _small_ensemble(enepara)
+    n = int(cx[0]["size"]["n_rep"])
+    ref = _oracle_run(oracle_lib, cx, 3, 120, spx=20)
+    with dock.Ensemble.from_complexes([cx], [3]) as ens:
+        ens.init()
+        ens.run(120, 20)
+        ens.sync()
+        got = ens.replicas(0)
+        st = ens.stats(0)
+    want = ref[0]["replica"][:n]
+    same = _same_trajectory(got, want)
+    # an acceptance decision can flip where FP32 and FP64 energies straddle the
+    # threshold; after that the chain legitimately differs.  Nearly all agree:
+    assert same.mean() >= 0.9, same.mean()
+    _close(got["energy"][same], want["energy"][same])
+    assert st[:, 2].sum() > 0, "no exchange attempted"
+    assert st[:, 3].sum() > 0, "no exchange accepted"
+
+
+def test_dock_drop_in_records(lib, enepara, oracle_lib):
+    """Dock(): initial energy, two dump chunks, Records of the last chunk, final
+    replicas copied back to the host Complex (backend_gpu.cu:63-133)."""
+    cx = _small_ensemble(enepara, seed=9)
+    cx[0]["mcpara"]["steps_total"] = 400
+    cx[0]["mcpara"]["steps_per_dump"] = 200
+    n = int(cx[0]["size"]["n_rep"])
+    ref = cx.copy()
+    rrec = Lo.aligned_zeros(Lo.RECORD, n)
+    oracle_lib.montecarlo(ref, rrec, 0, 1, 11)
+    oracle_lib.montecarlo(ref, rrec, 0, 200, 11)
+    oracle_lib.montecarlo(ref, rrec, 200, 200, 11)
+    work = cx.copy()
+    with dock.DockSession(1, seed=11) as s:
+        rec = s.dock(work)
+    same = _same_trajectory(work[0]["replica"][:n], ref[0]["replica"][:n])
+    assert same.mean() >= 0.9
+    for r in np.nonzero(same)[0]:
+        ne = int(rec[r]["next_entry"])
+        assert ne == int(rrec[r]["next_entry"])
+        got, want = rec[r]["replica"][:ne], rrec[r]["replica"][:ne]
+        np.testing.assert_array_equal(got["step"], want["step"])
+        assert np.all(got["step"] >= 200) and np.all(got["step"] < 400)
+        np.testing.assert_array_equal(got["movematrix"], want["movematrix"])
+        _close(got["energy"], want["energy"])
+        np.testing.assert_array_equal(got["is_accept"], want["is_accept"])
+    assert np.all(work[0]["replica"]["is_accept"][:n] == ref[0]["replica"]["is_accept"][:n])
+
+
+def test_dock_initial_energy_record(lib, enepara, oracle_lib):
+    """With one dump chunk, Record entry 0 is the initial state at step 0 -- the
+    entry the reference prints as its known-answer line (kernel_print.C:9-15)."""
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara, steps_total=200, steps_per_dump=200)
+    with dock.DockSession(1, seed=5) as s:
+        rec = s.dock(cx.copy())
+    e, _ = oracle_lib.energy(cx, 0, 0, np.zeros(6, np.float32))
+    first = rec[0]["replica"][0]
+    assert first["step"] == 0 and rec[0]["next_entry"] >= 1
+    assert np.all(np.abs(first["energy"] - e) <= 1e-5 * np.maximum(np.abs(e), 1.0))
+
+
+def test_plain_kernel_matches_batched(lib, enepara):
+    cx = _small_ensemble(enepara, seed=6)
+    res = {}
+    for kern in (0, 1):
+        check(lib.gd_set_option(b"kernel", kern))
+        try:
+            with dock.Ensemble.from_complexes([cx], [5]) as ens:
+                ens.init()
+                ens.run(100, 25)
+                ens.sync()
+                res[kern] = ens.replicas(0)
+        finally:
+            check(lib.gd_set_option(b"kernel", 0))
+    same = _same_trajectory(res[0], res[1])
+    assert same.mean() >= 0.9
+    _close(res[0]["energy"][same], res[1]["energy"][same], 2e-5)
+
+
+def test_reproducible_and_tile_independent(lib, enepara):
+    """Same seed -> bit-identical states, whatever the number of replicas per CTA."""
+    cx = _small_ensemble(enepara, seed=2)
+    out = []
+    for warps in (0, 3, 7):
+        check(lib.gd_set_option(b"warps", warps))
+        try:
+            with dock.Ensemble.from_complexes([cx], [21]) as ens:
+                ens.init()
+                ens.run(60, 15)
+                ens.sync()
+                out.append(ens.replicas(0))
+        finally:
+            check(lib.gd_set_option(b"warps", 0))
+    for o in out[1:]:
+        assert o.tobytes() == out[0].tobytes()
+
+
+def test_batch_independent(lib, enepara):
+    """A job's result is the same alone and batched with other jobs."""
+    cxa = _small_ensemble(enepara, seed=31, L=12)
+    cxb = _small_ensemble(enepara, seed=32, L=40, P=500)
+    with dock.Ensemble.from_complexes([cxa], [1]) as e1:
+        e1.init()
+        e1.run(40, 10)
+        e1.sync()
+        alone = e1.replicas(0)
+    with dock.Ensemble.from_complexes([cxb, cxa], [2, 1]) as e2:
+        e2.init()
+        e2.run(40, 10)
+        e2.sync()
+        mixed = e2.replicas(1)
+    assert alone.tobytes() == mixed.tobytes()
+
+
+def test_invalid_inputs_rejected(lib, enepara):
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara)
+    bad = cx.copy()
+    bad[0]["lig"][0]["t2"][0] = 40                  # ligand type outside 0..23
+    with pytest.raises(GdockError) as ei:
+        dock.Ensemble.from_complexes([bad], [1])
+    assert ei.value.code == GD_E_INVALID
+    bad = cx.copy()
+    bad[0]["mcs"][0]["x"][:] = Lo.MCS_INVALID_COORD   # an MCS row with no coordinate
+    with pytest.raises(GdockError):
+        dock.Ensemble.from_complexes([bad], [1])
