@@ -40,6 +40,7 @@ EXPORTED = [
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
+    "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
 ]
 
 
@@ -103,6 +104,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),
+        "gd_eval_poses_noalloc": (i, [vp, i, vp, vp, i, vp, vp, vp]), "gd_noalloc_scratch_bytes": (C.c_size_t, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

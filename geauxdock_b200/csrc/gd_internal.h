@@ -162,6 +162,10 @@ int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem)
 // mode 0: Monte Carlo chunk over the work items; mode 1: pose evaluation.
 cudaError_t launch_kernel(int mode, int precision, const TileConfig &tc, const KArgs &a, int grid, cudaStream_t st);
 
+// Pose evaluation reading the packed job from global memory (8 poses per 256-thread CTA, grid-stride).
+cudaError_t launch_eval_global(int precision, const DevJob *d_job, const int *conf, const float *mm, int n,
+                               float *out, float *raw, int *err, int grid, cudaStream_t st);
+
 // Replica-exchange sweep x of one job (ngroup = nprt * nlig groups of ntmp temperatures).
 cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cudaStream_t st);
 

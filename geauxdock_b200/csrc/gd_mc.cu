@@ -619,6 +619,56 @@ __global__ void exchange_kernel(const DevJob *jobp, int x)
   }
 }
 
+// Pose evaluation that reads the packed job straight from global memory (no
+// shared-memory staging, no work items): warp w of the grid evaluates poses
+// w, w + (number of warps), ...  Used by the allocation-free entry point.
+template <int PREC, int KPL, int AB>
+__global__ void __launch_bounds__(256) eval_global_kernel(const DevJob *jobp, const int *conf, const float *mm,
+                                                          int n, float *out, float *raw, int *err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (err != nullptr && *(volatile int *)err != 0) return;  // the job was not packed
+  const DevJob &J = *jobp;
+  const int warp = threadIdx.x >> 5, lane = lane_id();
+  const uint32_t lig_bytes = (uint32_t)kMaxAtoms * (PREC == kFP64 ? 32u : 16u);
+  unsigned char *wb = smem + (size_t)warp * (lig_bytes + sizeof(EnergyScratch));
+  EnergyScratch *esc = reinterpret_cast<EnergyScratch *>(wb + lig_bytes);
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < n; i += nwarps) {
+    const int ilig = conf[2 * i], iprt = conf[2 * i + 1];
+    if (ilig < 0 || ilig >= J.nlig || iprt < 0 || iprt >= J.nprt) {
+      if (lane < 10) out[10 * (size_t)i + lane] = __int_as_float(0x7fc00000);
+      if (lane == 0) atomicOr(err, kErrSize);
+      continue;
+    }
+    if (lane < 6) esc->mm[lane] = mm[6 * (size_t)i + lane];
+    __syncwarp();
+    const size_t P = (size_t)J.npoint_pad;
+    energy_warp<PREC, KPL, AB>(J, J.par, J.pos + iprt * P, J.aux + iprt * P, J.kde, J.ltype, wb, ilig, iprt, esc->mm,
+                               esc);
+    if (lane < 10) out[10 * (size_t)i + lane] = (float)esc->e[lane];
+    if (raw && lane < 9) raw[9 * (size_t)i + lane] = (float)esc->raw[lane];
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_eval_global(int precision, const DevJob *d_job, const int *conf, const float *mm, int n,
+                               float *out, float *raw, int *err, int grid, cudaStream_t st)
+{
+  const int threads = 256;
+  const size_t smem = (size_t)(threads / 32) * ((size_t)kMaxAtoms * (precision == kFP64 ? 32 : 16) + sizeof(EnergyScratch));
+  if (n <= 0) return cudaSuccess;
+  if (precision == kFP32)
+    eval_global_kernel<kFP32, 1, 8><<<grid, threads, smem, st>>>(d_job, conf, mm, n, out, raw, err);
+  else if (precision == kFP32Kahan)
+    eval_global_kernel<kFP32Kahan, 1, 8><<<grid, threads, smem, st>>>(d_job, conf, mm, n, out, raw, err);
+  else if (precision == kFP64)
+    eval_global_kernel<kFP64, 1, 8><<<grid, threads, smem, st>>>(d_job, conf, mm, n, out, raw, err);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------- launchers --
 size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision)
 {

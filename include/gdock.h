@@ -101,6 +101,27 @@ long long gd_get_option(const char *name);
 int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int precision, float *out,
                   double *out64, float *raw);
 
+/* Pose energies without any memory allocation.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc/cudaFree around a
+ * docking call: a process whose device memory belongs to another allocator
+ * (a framework's caching allocator, a pool reserved at start-up), or a
+ * latency-bound serving loop that cannot afford cudaFree's device-wide
+ * synchronisation.  Same result as gd_eval_poses, but every pointer is device
+ * memory the caller owns: d_complex is a reference-layout Complex (for
+ * example cd[g] after CopyH2D), d_conf[n][2] / d_mm[n][6] the poses,
+ * d_out[n][10] and d_raw[n][9] (may be NULL) the energies; stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call returns after
+ * the work on that stream finished.  The packed device layout goes into one
+ * fixed scratch array in the library (gd_noalloc_scratch_bytes(), about
+ * 5.6 MB, held on every GPU that loads the library until exit), sized for the
+ * reference Complex's caps: larger sizes fail with GD_E_CAPACITY.  The first
+ * call on a device looks up the scratch array's address; make that first
+ * call before any stream capture.  All calls on a device share the scratch
+ * array: calls whose GPU work overlaps race on it. */
+int gd_eval_poses_noalloc(const Complex *d_complex, int n, const int *d_conf, const float *d_mm, int precision,
+                          float *d_out, float *d_raw, void *stream);
+size_t gd_noalloc_scratch_bytes(void);
+
 /* OptimizeEnepara (src/frontend/util_optimize_soa.C:489-540): raw parameters
  * -> the precomputed tables of EnePara, bit-identical to the reference. */
 int gd_optimize_enepara(const EnePara0 *in, EnePara *out);
