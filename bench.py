@@ -57,6 +57,11 @@ def _args():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--mc-steps", type=int, default=STEPS_PER_INTERVAL,
+                   help="MC steps per bench step (= steps between exchange sweeps)")
+    p.add_argument("--tile", default="", help="warps,kpl,ab: fixed tile shape (skips the autotuner)")
+    p.add_argument("--skip-extras", action="store_true",
+                   help="only the timed batched kernel (for profiling): no plain kernel, e2e or CPU baseline")
     return p.parse_args()
 
 
@@ -220,14 +225,21 @@ def run_ours(args) -> None:
 
     # ---------------- resident ensemble, batched kernel
     check(lib.gd_set_option(b"kernel", 0))
+    if args.tile:
+        w, kpl, ab = (int(x) for x in args.tile.split(","))
+        check(lib.gd_set_option(b"warps", w))
+        check(lib.gd_set_option(b"kpl", kpl))
+        check(lib.gd_set_option(b"ab", ab))
+        args.no_autotune = True
     ens = dock.Ensemble.from_complexes([cx], [1000 + rank], device=local)
     ens.init()
     ens.sync()
     tune = "" if args.no_autotune else ens.autotune(4)
     stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    spi = args.mc_steps
     for _ in range(args.warmup):
-        ens.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+        ens.run(spi, spi)
     ens.sync()
     barrier()
     clocks = Clocks(local)
@@ -235,7 +247,7 @@ def run_ours(args) -> None:
     e0.record(stream)
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
-            ens.run(STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+            ens.run(spi, spi)
             flush.zero_()
     e1.record(stream)
     e1.synchronize()
@@ -247,14 +259,24 @@ def run_ours(args) -> None:
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    pose_evals = n_rep * STEPS_PER_INTERVAL * args.steps
+    pose_evals = n_rep * spi * args.steps
     value = world * pose_evals / (ms_max / 1e3)
     avg_launch_ms = kernel_ms / max(mc_launches, 1)
-    flops_per_launch = fpp * n_rep * STEPS_PER_INTERVAL
+    flops_per_launch = fpp * n_rep * spi
     peak = C.c_double()
     check(lib.gd_fp32_peak(C.byref(peak)))
     achieved = flops_per_launch / (avg_launch_ms / 1e3) / 1e12
     ens.close()
+    if args.skip_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "mc_steps_per_step": spi,
+                              "roofline": {"achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                                           "frac": achieved / peak.value, "avg_launch_ms": avg_launch_ms},
+                              "clocks": ck, "note": "profiling run (--skip-extras)"}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # ---------------- plain kernel, same work
     check(lib.gd_set_option(b"kernel", 1))

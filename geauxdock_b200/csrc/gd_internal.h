@@ -7,15 +7,17 @@
 // only the boundary format: it is packed once into compact structure-of-arrays
 // buffers sized to the actual problem:
 //
-//   pocket conformation  pos[P] float4 (x, y, z, ele), aux[P] float2 (hpp_eff, type)
+//   pocket conformation  pos[P] float4 (x, y, z, ele), aux[P] float2 (hpp_eff,
+//                        type): hydrophobic-contact points first, each part
 //                        sorted by point type, padded with inert points
 //   force-field tables   tab4[24][32] float4 (p1a, p2a, pmf0, pmf1)
-//                        tab2[24][32] float2 (hdb0, hdb1), unused pairs zeroed
+//                        tab2[24][32] float2 (scaled hdb1, hdb0), unused pairs zeroed
 //   ligand conformation  lig[L] float4 (x, y, z, charge), atoms grouped by type
 //   KDE points           kde[K] float4 (x, y, z, type), sorted by type, with
 //                        per-type ranges
 //   MCS templates        mcs[L][M] float4 (x, y, z, valid), atom-major
-//   pocket potential     psp[prt conf][24][P] pre-gathered per sorted point
+//   pocket potential     psp[prt conf][24][P] pre-gathered per sorted point,
+//                        pspmask[prt conf][P] its non-zero ligand types
 //
 // Every array a CTA stages into shared memory is a multiple of 16 bytes and
 // starts 16-byte aligned, so it can be copied with one 1-D bulk (TMA) copy.
@@ -34,17 +36,26 @@ constexpr int kPadType = 30;             // point type given to padding points
 constexpr int kMaxAtoms = 128;           // ligand atoms per job on the batched path
 constexpr int kPointAlign = 128;         // pocket conformations padded to this many points
 constexpr int kMaxTemps = GD_MAX_TMP;
-constexpr int kMaxCtaThreads = 512;       // launch bound of the batched kernel (<= 16 replica-warps)
+constexpr int kMaxCtaThreads = 512;
+// c = sqrt(log2(e) / 2): exp(-h^2/2) = 2^-(h c)^2 (scaled hydrogen-bond table entries)
+constexpr double kHdbC = 0.8493218002880191;       // launch bound of the batched kernel (<= 16 replica-warps)
 
 // Force-field parameters of one job, in the order the kernels stage them.
+// The FP32 pair code uses algebraically rearranged forms of the reference
+// formulas whose constants are precomputed here (values in the comments).
 struct alignas(16) DevParams {
   float4 tab4[kLigTypes][kTabCols];   // p1a, p2a, pmf0, pmf1
-  float2 tab2[kLigTypes][kTabCols];   // hdb0, hdb1 (both 0 where hdb0 <= 0.1)
+  float2 tab2[kLigTypes][kTabCols];   // hdb1*c, -hdb0*hdb1*c with c = sqrt(log2(e)/2);
+                                      // zero where hdb0 <= 0.1 (no hydrogen-bond parameters)
+  uint32_t hdbmask[kLigTypes];        // bit pt set where (ligand type, point type) has hdb0 > 0.1
   float hpl0[kLigTypes], hpl1[kLigTypes], hpl2[kLigTypes];
   float a_para[12], b_para[12], w[12];
   float lj0, lj1, el0, el1, inv_el1, a1, b1, kde2, kde3_inv;
+  float lj01;                         // lj0 * lj1
+  float ele_a, ele_b, ele_d2max;      // a1 el1^2, b1 el1^3, 1/el1^2 (near-field branch: d^2 < 1/el1^2)
+  float hdb_cinv;                     // 1/c
   float move_scale[6];
-  float pad_[1];
+  float pad_[2];
 };
 static_assert(sizeof(DevParams) % 16 == 0, "DevParams must be a multiple of 16 bytes");
 
@@ -69,15 +80,17 @@ struct DevJob {
   int nlig;                // ligand conformations
   int lstride;             // float4 stride between ligand conformations (>= L)
   const float4 *lig;       // [nlig][lstride] (x, y, z, charge), type-grouped order
-  const int *ltype;        // [L] atom type in type-grouped order
+  const int2 *lgrp;        // [L] (atom type, end index of its type group), type-grouped order
   const float *lcenter;    // [nlig][3] ligand centre in the lab frame
   // pocket
   int npoint_pad;          // padded point count (multiple of kPointAlign)
   int nprt;                // protein conformations
   const float4 *pos;       // [nprt][npoint_pad]
-  const float2 *aux;       // [nprt][npoint_pad]
+  const float2 *aux;       // [nprt][npoint_pad] (hpp if cdc == 1 else 0, point type)
+  const int *ncdc;         // [nprt] hydrophobic-contact (cdc == 1) points, placed first in each conformation
   const float *pcenter;    // [nprt][3] pocket centre
   const float *psp;        // [nprt][24][npoint_pad]
+  const uint32_t *pspmask; // [nprt][npoint_pad] bit t set where psp[.][t][p] != 0
   // KDE
   int nkde;
   const float4 *kde;       // [nkde]
@@ -92,6 +105,7 @@ struct DevJob {
   const float *minus_beta; // [ntmp]
   // parameters
   const DevParams *par;
+  const float2 *hdbref;    // [24][32] (hdb0, hdb1) as in EnePara, zero where hdb0 <= 0.1 (FP64 kernels)
   // replicas (layout of the reference's replica array: index
   // n_tmp*n_lig*p + n_lig*t + l, src/frontend/util.C:380)
   int nrep;

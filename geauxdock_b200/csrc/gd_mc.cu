@@ -57,7 +57,7 @@ __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 // ----------------------------------------------------------- smem layout --
 struct SmemLayout {
-  uint32_t params, ltype, pos, aux, kde, warp0, warp_bytes, lig_bytes, total;
+  uint32_t params, lgrp, pos, aux, kde, warp0, warp_bytes, lig_bytes, total;
 };
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
@@ -68,8 +68,8 @@ __host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots,
   uint32_t off = 0;
   s.params = off;
   off = align16(off + (uint32_t)sizeof(DevParams));
-  s.ltype = off;
-  off = align16(off + (uint32_t)sizeof(int) * kMaxAtoms);
+  s.lgrp = off;
+  off = align16(off + (uint32_t)sizeof(int2) * kMaxAtoms);
   s.pos = off;
   off = align16(off + 16u * (uint32_t)P);
   s.aux = off;
@@ -98,11 +98,102 @@ struct EnergyScratch {
 };
 static_assert(sizeof(EnergyScratch) == 192, "EnergyScratch size is part of the smem layout");
 
+// Running sums of the pair terms of one point row.
+template <typename T>
+struct PairAcc {
+  T vdw, ele, pmf, psp, hdb;
+};
+
+// Scalar force-field constants of the pair terms, read once per pose.
+struct PairConst {
+  float lj0, lj1, lj01, el0, el1, inv_el1, a1, b1, ea, eb, ed2;
+  __device__ static PairConst load(const DevParams *p)
+  {
+    PairConst c;
+    c.lj0 = p->lj0; c.lj1 = p->lj1; c.lj01 = p->lj01; c.el0 = p->el0; c.el1 = p->el1; c.inv_el1 = p->inv_el1;
+    c.a1 = p->a1; c.b1 = p->b1; c.ea = p->ele_a; c.eb = p->ele_b; c.ed2 = p->ele_d2max;
+    return c;
+  }
+};
+
+// Pair terms of ligand atoms [a, aend) (one type group) against the lane's
+// KPL points, energy_prt_v1.cu:56-139 except the hydrophobic contact.  HDB /
+// PSP: evaluate the hydrogen-bond / pocket-specific terms (some lane has a
+// non-zero parameter).  FP32 uses rearranged forms of the same formulas:
+//   p1 = p1a r^9, p2 = p2a r^6 with r = 1/d (one rsqrt),
+//   p4 = p1 (lj0 + lj0 lj1 d^2) + 1,
+//   g  = el0 + d^2 (a1 el1^2 + b1 el1^3 d) for el1 d < 1, else r/el1,
+//   hdb1 exp(-((d - hdb0) hdb1)^2 / 2) = (hdb1 c) 2^-(d hdb1 c - hdb0 hdb1 c)^2 / c
+// (t2 = (hdb1 c, -hdb0 hdb1 c); the FP64 kernel gets t2 = (hdb0, hdb1)).
+template <int PREC, int KPL, bool HDB, bool PSP, typename T>
+__device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, const T (&px)[KPL],
+                                           const T (&py)[KPL], const T (&pz)[KPL], const T (&pe)[KPL],
+                                           const float4 (&t4)[KPL], const float2 (&t2)[KPL], const T (&tps)[KPL],
+                                           const PairConst &c, PairAcc<T> &acc)
+{
+  if constexpr (PREC == kFP64) {
+    const double lj0 = c.lj0, lj1 = c.lj1, el0 = c.el0, el1 = c.el1, a1 = c.a1, b1 = c.b1;
+    for (; a < aend; ++a) {
+      const V4<double> la = lig[a];
+#pragma unroll
+      for (int j = 0; j < KPL; ++j) {
+        const double dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double d4 = d2 * d2;
+        const double d = sqrt(d2);
+        const double p1 = (double)t4[j].x / (d4 * d4 * d);
+        const double p2 = (double)t4[j].y / (d4 * d2);
+        const double p4 = p1 * lj0 * (1.0 + lj1 * d2) + 1.0;
+        acc.vdw += (p1 - p2) / p4;
+        const double s1 = el1 * d;
+        const double g = (s1 < 1.0) ? el0 + a1 * s1 * s1 + b1 * s1 * s1 * s1 : 1.0 / s1;
+        acc.ele += la.w * pe[j] * g;
+        const double dmp = d - (double)t4[j].z;
+        acc.pmf += (double)t4[j].w / (1.0 + exp((-0.5 * d + 6.0) * dmp));
+        if constexpr (PSP) acc.psp += (dmp <= 0.0) ? tps[j] : 0.0;
+        if constexpr (HDB) {
+          const double h3 = (d - (double)t2[j].x) * (double)t2[j].y;
+          acc.hdb += (double)t2[j].y * exp(-0.5 * h3 * h3);
+        }
+      }
+    }
+  } else {
+#pragma unroll 2
+    for (; a < aend; ++a) {
+      const V4<float> la = lig[a];
+#pragma unroll
+      for (int j = 0; j < KPL; ++j) {
+        const float dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float r = rsqrt_approx(d2);
+        const float d = d2 * r;
+        const float r2 = r * r;
+        const float r3 = r2 * r;
+        const float r6 = r3 * r3;
+        const float p1 = t4[j].x * (r6 * r3);
+        const float p2 = t4[j].y * r6;
+        const float p4 = fmaf(p1, fmaf(c.lj01, d2, c.lj0), 1.0f);
+        acc.vdw = fmaf(p1 - p2, rcp_approx(p4), acc.vdw);
+        const float g = (d2 < c.ed2) ? fmaf(d2, fmaf(c.eb, d, c.ea), c.el0) : r * c.inv_el1;
+        acc.ele = fmaf(la.w * pe[j], g, acc.ele);
+        const float dmp = d - t4[j].z;
+        const float ex = ex2_approx(fmaf(-0.5f * kLog2e, d, 6.0f * kLog2e) * dmp);
+        acc.pmf = fmaf(t4[j].w, rcp_approx(1.0f + ex), acc.pmf);
+        if constexpr (PSP) acc.psp += (dmp <= 0.0f) ? tps[j] : 0.0f;
+        if constexpr (HDB) {
+          const float h = fmaf(d, t2[j].x, t2[j].y);
+          acc.hdb = fmaf(t2[j].x, ex2_approx(-(h * h)), acc.hdb);
+        }
+      }
+    }
+  }
+}
+
 template <int PREC, int KPL, int AB>
 __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__restrict__ par,
                                          const float4 *__restrict__ pos, const float2 *__restrict__ aux,
-                                         const float4 *__restrict__ kde, const int *__restrict__ ltype, void *ligbuf,
-                                         int ilig, int iprt, const float *mm, EnergyScratch *out)
+                                         const float4 *__restrict__ kde, const int2 *__restrict__ lgrp,
+                                         void *ligbuf, int ilig, int iprt, const float *mm, EnergyScratch *out)
 {
   using T = typename std::conditional<PREC == kFP64, double, float>::type;
   const int lane = lane_id();
@@ -148,130 +239,137 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   __syncwarp();
 
   // ---- protein-ligand pair terms, energy_prt_v1.cu:8-174
-  const T lj0 = par->lj0, lj1 = par->lj1, el0 = par->el0, el1 = par->el1, inv_el1 = par->inv_el1;
-  const T a1 = par->a1, b1 = par->b1;
+  // Pass 1: every term but the hydrophobic contact.  Lane i holds points
+  // row + i + 32 j (j < KPL); atoms are visited one type group at a time, with
+  // the (atom type, point type) table entries loaded once per group.  The
+  // hydrogen-bond and pocket-specific terms are skipped for a group when no
+  // lane of the warp has a non-zero parameter for it (both are sparse).
   T s_vdw = 0, s_ele = 0, s_pmf = 0, s_psp = 0, s_hdb = 0;
   float c_vdw = 0.f, c_ele = 0.f, c_pmf = 0.f, c_psp = 0.f, c_hdb = 0.f;  // Kahan compensations
-  T ehpc = 0;
   const float *pspc = J.psp + (size_t)iprt * kLigTypes * P;
+  const uint32_t *pmc = J.pspmask + (size_t)iprt * P;
+  const PairConst kc = PairConst::load(par);
 
-  for (int a0 = 0; a0 < L; a0 += AB) {
-    T hpc[AB];
+  for (int row = 0; row < P; row += 32 * KPL) {
+    T px[KPL], py[KPL], pz[KPL], pe[KPL];
+    int pt[KPL];
+    uint32_t pm[KPL];
 #pragma unroll
-    for (int k = 0; k < AB; ++k) hpc[k] = 0;
-
-    for (int row = 0; row < P; row += 32 * KPL) {
-      T px[KPL], py[KPL], pz[KPL], pe[KPL], ph[KPL];
-      int pt[KPL];
+    for (int j = 0; j < KPL; ++j) {
+      const int p = row + 32 * j + lane;
+      const float4 q = pos[p];
+      px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
+      pt[j] = __float_as_int(aux[p].y);
+      pm[j] = __ldg(pmc + p);
+    }
+    PairAcc<T> acc{0, 0, 0, 0, 0};
+    int a = 0;
+    while (a < L) {
+      const int2 grp = lgrp[a];
+      const int lt = grp.x, aend = grp.y;
+      const uint32_t hm = par->hdbmask[lt];
+      float4 t4[KPL];
+      float2 t2[KPL];
+      T tps[KPL];
+      bool any_hdb = false, any_psp = false;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
-        const int p = row + 32 * j + lane;
-        const float4 q = pos[p];
-        const float2 w = aux[p];
-        px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
-        ph[j] = w.x;
-        pt[j] = __float_as_int(w.y);
+        t4[j] = par->tab4[lt][pt[j]];
+        t2[j] = make_float2(0.f, 0.f);
+        tps[j] = 0;
+        any_hdb |= ((hm >> pt[j]) & 1u) != 0u;
+        any_psp |= ((pm[j] >> lt) & 1u) != 0u;
       }
-      T t_p1a[KPL], t_p2a[KPL], t_pmf0[KPL], t_pmf1[KPL], t_hdb0[KPL], t_hdb1[KPL], t_psp[KPL];
-      int cur = -1;
-      T b_vdw = 0, b_ele = 0, b_pmf = 0, b_psp = 0, b_hdb = 0;
+      any_hdb = __any_sync(0xffffffffu, any_hdb);
+      any_psp = __any_sync(0xffffffffu, any_psp);
+      if (any_hdb) {
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+          if constexpr (PREC == kFP64) t2[j] = __ldg(J.hdbref + lt * kTabCols + pt[j]);
+          else t2[j] = par->tab2[lt][pt[j]];
+        }
+      }
+      if (any_psp) {
+#pragma unroll
+        for (int j = 0; j < KPL; ++j)
+          if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+      }
+      if (any_hdb) {
+        if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+        else pair_atoms<PREC, KPL, true, false>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+      } else {
+        if (any_psp) pair_atoms<PREC, KPL, false, true>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+        else pair_atoms<PREC, KPL, false, false>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+      }
+      a = aend;
+    }
+    if constexpr (PREC == kFP32Kahan) {
+      kahan_add(s_vdw, c_vdw, acc.vdw);
+      kahan_add(s_ele, c_ele, acc.ele);
+      kahan_add(s_pmf, c_pmf, acc.pmf);
+      kahan_add(s_psp, c_psp, acc.psp);
+      kahan_add(s_hdb, c_hdb, acc.hdb);
+    } else {
+      s_vdw += acc.vdw;
+      s_ele += acc.ele;
+      s_pmf += acc.pmf;
+      s_psp += acc.psp;
+      s_hdb += acc.hdb;
+    }
+  }
 
+  // Pass 2: hydrophobic contact (energy_prt_v1.cu:42-49) over the rows that
+  // hold cdc == 1 points (placed first).  The polynomial
+  // 1 - 3.5x + 4.5x^2 - 2.5x^3 + 0.5x^4 (x = d^2/81) is (1-x)^3 (1-x/2);
+  // clamping 1-x at 0 applies the d^2 <= 81 cut-off.  Per-atom sums stay in
+  // registers for AB atoms at a time, then the per-atom restraint
+  // (energy_prt_v1.cu:162-169).
+  T ehpc = 0;
+  {
+    const int rows = ((J.ncdc[iprt] + 32 * KPL - 1) / (32 * KPL)) * (32 * KPL);
+    for (int a0 = 0; a0 < L; a0 += AB) {
+      T hpc[AB];
+#pragma unroll
+      for (int k = 0; k < AB; ++k) hpc[k] = 0;
+      for (int row = 0; row < rows; row += 32 * KPL) {
+        T px[KPL], py[KPL], pz[KPL], ph[KPL];
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+          const int p = row + 32 * j + lane;
+          const float4 q = pos[p];
+          px[j] = q.x; py[j] = q.y; pz[j] = q.z;
+          ph[j] = aux[p].x;
+        }
+#pragma unroll
+        for (int k = 0; k < AB; ++k) {
+          const int a = a0 + k;
+          if (a >= L) break;
+          const V4<T> la = lig[a];
+#pragma unroll
+          for (int j = 0; j < KPL; ++j) {
+            const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
+            const T d2 = dx * dx + dy * dy + dz * dz;
+            T t, u;
+            if constexpr (PREC == kFP64) {
+              t = fmax(1.0 - d2 / 81.0, 0.0);
+              u = 1.0 - 0.5 * d2 / 81.0;
+            } else {
+              t = fmaxf(fmaf(d2, -1.0f / 81.0f, 1.0f), 0.0f);
+              u = fmaf(d2, -0.5f / 81.0f, 1.0f);
+            }
+            hpc[k] += ph[j] * (t * t * t * u);
+          }
+        }
+      }
 #pragma unroll
       for (int k = 0; k < AB; ++k) {
         const int a = a0 + k;
         if (a >= L) break;
-        const V4<T> la = lig[a];
-        const int lt = ltype[a];
-        if (lt != cur) {
-          cur = lt;
-#pragma unroll
-          for (int j = 0; j < KPL; ++j) {
-            const float4 t4 = par->tab4[lt][pt[j]];
-            const float2 t2 = par->tab2[lt][pt[j]];
-            t_p1a[j] = t4.x; t_p2a[j] = t4.y; t_pmf0[j] = t4.z; t_pmf1[j] = t4.w;
-            t_hdb0[j] = t2.x; t_hdb1[j] = t2.y;
-            t_psp[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < KPL; ++j) {
-          const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
-          const T d2 = dx * dx + dy * dy + dz * dz;
-          T r;
-          if constexpr (PREC == kFP64) r = rsqrt(d2);
-          else r = rsqrt_approx(d2);
-          const T d = d2 * r;
-
-          // hydrophobic contact (cdc == 1 folded into hpp_eff), energy_prt_v1.cu:42-49
-          const T poly = (((T)kH4 * d2 + (T)kH3) * d2 + (T)kH2) * d2 + (T)kH1;
-          const T hp = poly * d2 + (T)1;
-          hpc[k] += (d2 <= (T)81) ? ph[j] * hp : (T)0;
-
-          // Lennard-Jones, energy_prt_v1.cu:60-63: p1 = p1a/d^9, p2 = p2a/d^6
-          const T r2 = r * r;
-          const T r3 = r2 * r;
-          const T r6 = r3 * r3;
-          const T p1 = t_p1a[j] * (r6 * r3);
-          const T p2 = t_p2a[j] * r6;
-          const T p4 = p1 * lj0 * ((T)1 + lj1 * d2) + (T)1;
-          T inv_p4;
-          if constexpr (PREC == kFP64) inv_p4 = 1.0 / p4;
-          else inv_p4 = rcp_approx(p4);
-          b_vdw += (p1 - p2) * inv_p4;
-
-          // electrostatics, energy_prt_v1.cu:81-85
-          const T s1 = el1 * d;
-          const T g_near = el0 + s1 * s1 * (a1 + b1 * s1);
-          const T g_far = r * inv_el1;
-          const T g1 = (s1 < (T)1) ? g_near : g_far;
-          b_ele += la.w * pe[j] * g1;
-
-          // contact (pmf) sigmoid, energy_prt_v1.cu:95-97
-          const T dmp = d - t_pmf0[j];
-          T ex, inv_den;
-          if constexpr (PREC == kFP64) {
-            ex = exp((-0.5 * d + 6.0) * dmp);
-            inv_den = 1.0 / (1.0 + ex);
-          } else {
-            ex = ex2_approx(((-0.5f * kLog2e) * d + 6.0f * kLog2e) * dmp);
-            inv_den = rcp_approx(1.0f + ex);
-          }
-          b_pmf += t_pmf1[j] * inv_den;
-
-          // pocket-specific potential (c == 2 folded into t_psp), energy_prt_v1.cu:109-115
-          b_psp += (dmp <= (T)0) ? t_psp[j] : (T)0;
-
-          // hydrogen bond (hdb0 <= 0.1 folded into hdb1 = 0), energy_prt_v1.cu:133-138
-          const T h3 = (d - t_hdb0[j]) * t_hdb1[j];
-          T g;
-          if constexpr (PREC == kFP64) g = exp(-0.5 * h3 * h3);
-          else g = ex2_approx((-0.5f * kLog2e) * h3 * h3);
-          b_hdb += t_hdb1[j] * g;
-        }
+        const T S = warp_sum(hpc[k]);
+        const int lt = lgrp[a].x;
+        const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
+        ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
       }
-      if constexpr (PREC == kFP32Kahan) {
-        kahan_add(s_vdw, c_vdw, b_vdw);
-        kahan_add(s_ele, c_ele, b_ele);
-        kahan_add(s_pmf, c_pmf, b_pmf);
-        kahan_add(s_psp, c_psp, b_psp);
-        kahan_add(s_hdb, c_hdb, b_hdb);
-      } else {
-        s_vdw += b_vdw;
-        s_ele += b_ele;
-        s_pmf += b_pmf;
-        s_psp += b_psp;
-        s_hdb += b_hdb;
-      }
-    }
-    // hydrophobic restraint per atom, energy_prt_v1.cu:162-169
-#pragma unroll
-    for (int k = 0; k < AB; ++k) {
-      const int a = a0 + k;
-      if (a >= L) break;
-      const T S = warp_sum(hpc[k]);
-      const int lt = ltype[a];
-      const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
-      ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
     }
   }
 
@@ -289,6 +387,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     psp = warp_sum(s_psp);
     hdb = warp_sum(s_hdb);
   }
+  // the FP32 hydrogen-bond sum carries the table's factor c (see DevParams)
+  if constexpr (PREC != kFP64) hdb *= par->hdb_cinv;
 
   // ---- KDE, energy_kde_v1.cu:183-274: per atom, mean of exp(kde2 d^2) over
   // the KDE points of the same type; atoms with no such point contribute 0.
@@ -296,7 +396,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   {
     const T kde2 = par->kde2;
     for (int a = 0; a < L; ++a) {
-      const int lt = ltype[a];
+      const int lt = lgrp[a].x;
       const int cnt = J.kcnt[lt];
       if (cnt == 0) continue;
       const int beg = J.kbeg[lt];
@@ -395,8 +495,8 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
     bulk_g2s(smem + sl.aux, J.aux + (size_t)wi.prt * P, 8u * (uint32_t)P, bar);
     if (kde_in_smem && J.nkde > 0) bulk_g2s(smem + sl.kde, J.kde, 16u * (uint32_t)J.nkde, bar);
   }
-  int *lt = reinterpret_cast<int *>(smem + sl.ltype);
-  for (int a = threadIdx.x; a < J.natom; a += blockDim.x) lt[a] = J.ltype[a];
+  int2 *lg = reinterpret_cast<int2 *>(smem + sl.lgrp);
+  for (int a = threadIdx.x; a < J.natom; a += blockDim.x) lg[a] = J.lgrp[a];
   const bool ok = mbar_wait(bar, phase, kWaitLimit);
   phase ^= 1u;
   return ok;
@@ -447,7 +547,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     const float4 *pos = reinterpret_cast<const float4 *>(smem + sl.pos);
     const float2 *aux = reinterpret_cast<const float2 *>(smem + sl.aux);
     const float4 *kde = (J.nkde <= A.Kst) ? reinterpret_cast<const float4 *>(smem + sl.kde) : J.kde;
-    const int *ltype = reinterpret_cast<const int *>(smem + sl.ltype);
+    const int2 *lgrp = reinterpret_cast<const int2 *>(smem + sl.lgrp);
     unsigned char *wbase = smem + sl.warp0 + (size_t)warp * sl.warp_bytes;
     void *ligbuf = wbase;
     ReplicaMC *srep = reinterpret_cast<ReplicaMC *>(wbase + sl.lig_bytes);
@@ -461,7 +561,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         const int ilig = A.conf[2 * r], iprt = A.conf[2 * r + 1];
         if (lane < 6) esc->mm[lane] = A.mm[6 * r + lane];
         __syncwarp();
-        energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, ltype, ligbuf, ilig, iprt, esc->mm, esc);
+        energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, ligbuf, ilig, iprt, esc->mm, esc);
         if (lane < 10) {
           A.out[10 * (size_t)r + lane] = (float)esc->e[lane];
           if (A.out64) A.out64[10 * (size_t)r + lane] = esc->e[lane];
@@ -524,7 +624,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
             esc->mm[lane] = __fmaf_rn(par->move_scale[lane], 0.0f, srep->movematrix[lane]);
           }
           __syncwarp();
-          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, ltype, ligbuf, ilig, iprt, esc->mm, esc);
+          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, ligbuf, ilig, iprt, esc->mm, esc);
           const float etot = (float)esc->e[9];
 
           // Metropolis test in FP64, kernel_cuda_l1_montecarlo.cu:485-507
@@ -644,7 +744,7 @@ __global__ void __launch_bounds__(256) eval_global_kernel(const DevJob *jobp, co
     if (lane < 6) esc->mm[lane] = mm[6 * (size_t)i + lane];
     __syncwarp();
     const size_t P = (size_t)J.npoint_pad;
-    energy_warp<PREC, KPL, AB>(J, J.par, J.pos + iprt * P, J.aux + iprt * P, J.kde, J.ltype, wb, ilig, iprt, esc->mm,
+    energy_warp<PREC, KPL, AB>(J, J.par, J.pos + iprt * P, J.aux + iprt * P, J.kde, J.lgrp, wb, ilig, iprt, esc->mm,
                                esc);
     if (lane < 10) out[10 * (size_t)i + lane] = (float)esc->e[lane];
     if (raw && lane < 9) raw[9 * (size_t)i + lane] = (float)esc->raw[lane];

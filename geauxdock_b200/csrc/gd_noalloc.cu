@@ -41,7 +41,9 @@ struct NoAllocScratch {
   int err;        // nonzero: the call failed (cleared at the start of every call)
   int info[3];    // first failure: kind, field id, value
   int ltype[GD_MAXLIG];
+  int2 lgrp[GD_MAXLIG];
   int perm[GD_MAXLIG];
+  int ncdc[GD_MAX_CONF_PRT];
   float lcenter[GD_MAX_CONF_LIG * 3];
   float pcenter[GD_MAX_CONF_PRT * 3];
   float tcc[GD_MAX_MCS_ROW];
@@ -51,6 +53,8 @@ struct NoAllocScratch {
   float4 pos[GD_MAX_CONF_PRT * GD_MAXPRO];
   float2 aux[GD_MAX_CONF_PRT * GD_MAXPRO];
   float psp[GD_MAX_CONF_PRT * kLigTypes * GD_MAXPRO];
+  uint32_t pspmask[GD_MAX_CONF_PRT * GD_MAXPRO];
+  float2 hdbref[kLigTypes * kTabCols];
 };
 
 // field ids reported in info[1]
@@ -139,16 +143,24 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     const int lt = q / kTabCols, pt = q % kTabCols;
     if (pt < kPadType) {
       par.tab4[lt][pt] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
-      par.tab2[lt][pt] = ep.hdb0[lt][pt] > 0.1f ? make_float2(ep.hdb0[lt][pt], ep.hdb1[lt][pt]) : make_float2(0.f, 0.f);
+      const float h0 = ep.hdb0[lt][pt], h1 = ep.hdb1[lt][pt];
+      const bool on = h0 > 0.1f;
+      par.tab2[lt][pt] = on ? make_float2((float)((double)h1 * kHdbC), (float)(-(double)h0 * (double)h1 * kHdbC))
+                            : make_float2(0.f, 0.f);
+      S->hdbref[q] = on ? make_float2(h0, h1) : make_float2(0.f, 0.f);
     } else {
       par.tab4[lt][pt] = make_float4(0.f, 0.f, 0.f, 0.f);
       par.tab2[lt][pt] = make_float2(0.f, 0.f);
+      S->hdbref[q] = make_float2(0.f, 0.f);
     }
   }
   for (int q = tid; q < kLigTypes; q += blockDim.x) {
     par.hpl0[q] = ep.hpl0[q];
     par.hpl1[q] = ep.hpl1[q];
     par.hpl2[q] = ep.hpl2[q];
+    uint32_t m = 0;
+    for (int pt = 0; pt < kPadType; ++pt) m |= (ep.hdb0[q][pt] > 0.1f ? 1u : 0u) << pt;
+    par.hdbmask[q] = m;
   }
   for (int q = tid; q < 12; q += blockDim.x) {
     par.a_para[q] = q < GD_MAXWEI ? ep.a_para[q] : 0.f;
@@ -165,8 +177,13 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     par.b1 = ep.b1;
     par.kde2 = ep.kde2;
     par.kde3_inv = 1.0f / ep.kde3;
+    par.lj01 = (float)((double)ep.lj0 * ep.lj1);
+    par.ele_a = (float)((double)ep.a1 * ep.el1 * ep.el1);
+    par.ele_b = (float)((double)ep.b1 * ep.el1 * ep.el1 * ep.el1);
+    par.ele_d2max = (float)(1.0 / ((double)ep.el1 * ep.el1));
+    par.hdb_cinv = (float)(1.0 / kHdbC);
     for (int i = 0; i < 6; ++i) par.move_scale[i] = cx->mcpara.move_scale[i];
-    par.pad_[0] = 0.f;
+    par.pad_[0] = par.pad_[1] = 0.f;
     // ligand atoms grouped by type, stable (the host packer's order)
     int k = 0;
     for (int t = 0; t < kLigTypes; ++t)
@@ -176,6 +193,11 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
           S->ltype[k] = t;
           ++k;
         }
+    int end = L;
+    for (int a = L - 1; a >= 0; --a) {
+      if (a + 1 < L && S->ltype[a + 1] != S->ltype[a]) end = a + 1;
+      S->lgrp[a] = make_int2(S->ltype[a], end);
+    }
   }
   for (int q = tid; q < nlig * 3; q += blockDim.x) S->lcenter[q] = cx->lig[q / 3].center[q % 3];
   for (int q = tid; q < nprt * 3; q += blockDim.x) S->pcenter[q] = cx->prt[q / 3].pocket_center[q % 3];
@@ -220,14 +242,16 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     J.nlig = nlig;
     J.lstride = (L + 3) & ~3;
     J.lig = S->lig;
-    J.ltype = S->ltype;
+    J.lgrp = S->lgrp;
     J.lcenter = S->lcenter;
     J.npoint_pad = ((s_P + kPointAlign - 1) / kPointAlign) * kPointAlign;
     J.nprt = nprt;
     J.pos = S->pos;
     J.aux = S->aux;
+    J.ncdc = S->ncdc;
     J.pcenter = S->pcenter;
     J.psp = S->psp;
+    J.pspmask = S->pspmask;
     int nk = 0;
     for (int t = 0; t < kLigTypes; ++t) {
       J.kbeg[t] = s_kbeg[t];
@@ -242,6 +266,7 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     J.ntmp = 0;
     J.minus_beta = nullptr;
     J.par = &S->par;
+    J.hdbref = S->hdbref;
     J.nrep = 0;
     J.rep = nullptr;
     J.run_acc = nullptr;
@@ -253,51 +278,66 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
   }
 }
 
-// One CTA per protein conformation, one warp per point type: points sorted by
-// type (stable), padded with inert points, pocket-specific potential gathered.
+// One CTA per protein conformation.  Points are ordered as the host packer
+// orders them: hydrophobic-contact (cdc == 1) points first, each part sorted
+// by point type (stable); 60 buckets (cdc, type), two per warp, counted and
+// scattered with warp ballots.  Padding with inert points; pocket-specific
+// potential gathered with its non-zero type mask.
 __global__ void __launch_bounds__(1024) na_pocket_kernel(const Complex *__restrict__ cx, NoAllocScratch *S)
 {
-  __shared__ int s_cnt[32], s_beg[32];
+  constexpr int kBuckets = 2 * kPadType;
+  __shared__ int s_cnt[kBuckets], s_beg[kBuckets];
   if (S->err) return;
   const int i = blockIdx.x;
   const DevJob &J = S->job;
   if (i >= J.nprt) return;
   const Protein &pr = cx->prt[i];
   const int np = pr.prt_npoint, Pp = J.npoint_pad;
-  const int lane = threadIdx.x & 31, t = threadIdx.x >> 5;   // warp t handles point type t
-  if (t < kPadType) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  auto bucket = [&](int k) { return (pr.cdc[k] == 1 ? 0 : kPadType) + pr.t[k]; };
+  for (int bk = warp; bk < kBuckets; bk += nwarps) {
     int cnt = 0;
     for (int k0 = 0; k0 < np; k0 += 32) {
       const int k = k0 + lane;
-      cnt += __popc(__ballot_sync(0xffffffffu, k < np && pr.t[k] == t));
+      cnt += __popc(__ballot_sync(0xffffffffu, k < np && bucket(k) == bk));
     }
-    if (lane == 0) s_cnt[t] = cnt;
+    if (lane == 0) s_cnt[bk] = cnt;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     int b = 0;
-    for (int q = 0; q < kPadType; ++q) {
+    for (int q = 0; q < kBuckets; ++q) {
       s_beg[q] = b;
       b += s_cnt[q];
     }
+    int nc = 0;
+    for (int q = 0; q < kPadType; ++q) nc += s_cnt[q];
+    S->ncdc[i] = nc;
   }
   __syncthreads();
   float4 *pos = S->pos + (size_t)i * Pp;
   float2 *aux = S->aux + (size_t)i * Pp;
   float *psp = S->psp + (size_t)i * kLigTypes * Pp;
-  if (t < kPadType) {
-    int at = s_beg[t];
+  uint32_t *pm = S->pspmask + (size_t)i * Pp;
+  for (int bk = warp; bk < kBuckets; bk += nwarps) {
+    int at = s_beg[bk];
     for (int k0 = 0; k0 < np; k0 += 32) {
       const int k = k0 + lane;
-      const bool m = k < np && pr.t[k] == t;
+      const bool m = k < np && bucket(k) == bk;
       const unsigned b = __ballot_sync(0xffffffffu, m);
       if (m) {
         const int j = at + __popc(b & ((1u << lane) - 1u));
         pos[j] = make_float4(pr.x[k], pr.y[k], pr.z[k], pr.ele[k]);
-        aux[j] = make_float2(pr.cdc[k] == 1 ? pr.hpp[k] : 0.f, na_as_float(t));
+        aux[j] = make_float2(pr.cdc[k] == 1 ? pr.hpp[k] : 0.f, na_as_float(pr.t[k]));
         const bool c2 = pr.c[k] == 2;
         const int col = pr.seq3r[k];
-        for (int lt = 0; lt < kLigTypes; ++lt) psp[(size_t)lt * Pp + j] = c2 ? cx->psp.psp[lt][col] : 0.f;
+        uint32_t mask = 0;
+        for (int lt = 0; lt < kLigTypes; ++lt) {
+          const float v = c2 ? cx->psp.psp[lt][col] : 0.f;
+          psp[(size_t)lt * Pp + j] = v;
+          mask |= (v != 0.f ? 1u : 0u) << lt;
+        }
+        pm[j] = mask;
       }
       at += __popc(b);
     }
@@ -305,6 +345,7 @@ __global__ void __launch_bounds__(1024) na_pocket_kernel(const Complex *__restri
   for (int j = np + threadIdx.x; j < Pp; j += blockDim.x) {
     pos[j] = make_float4(1.0e4f + (float)j, 1.0e4f, 1.0e4f, 0.f);
     aux[j] = make_float2(0.f, na_as_float(kPadType));
+    pm[j] = 0u;
     for (int lt = 0; lt < kLigTypes; ++lt) psp[(size_t)lt * Pp + j] = 0.f;
   }
 }

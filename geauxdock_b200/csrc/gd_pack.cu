@@ -288,14 +288,18 @@ int job_from_desc(const gd_job_desc_t &d, int nprt, JobData &jd)
 void build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
 {
   std::memset(&p, 0, sizeof(p));
+  const double c = kHdbC;
   for (int lt = 0; lt < kLigTypes; ++lt) {
     for (int pt = 0; pt < GD_MAXTP1 && pt < kPadType; ++pt) {
       p.tab4[lt][pt] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
       // energy_prt_v1.cu:133-138 evaluates the hydrogen-bond term only where hdb0 > 0.1
-      if (ep.hdb0[lt][pt] > 0.1f)
-        p.tab2[lt][pt] = make_float2(ep.hdb0[lt][pt], ep.hdb1[lt][pt]);
-      else
+      const float h0 = ep.hdb0[lt][pt], h1 = ep.hdb1[lt][pt];
+      if (h0 > 0.1f) {
+        p.tab2[lt][pt] = make_float2((float)((double)h1 * c), (float)(-(double)h0 * (double)h1 * c));
+        p.hdbmask[lt] |= 1u << pt;
+      } else {
         p.tab2[lt][pt] = make_float2(0.f, 0.f);
+      }
     }
     p.hpl0[lt] = ep.hpl0[lt];
     p.hpl1[lt] = ep.hpl1[lt];
@@ -315,6 +319,11 @@ void build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
   p.b1 = ep.b1;
   p.kde2 = ep.kde2;
   p.kde3_inv = 1.0f / ep.kde3;  // kernel_cuda_l1_montecarlo.cu:194
+  p.lj01 = (float)((double)ep.lj0 * ep.lj1);
+  p.ele_a = (float)((double)ep.a1 * ep.el1 * ep.el1);
+  p.ele_b = (float)((double)ep.b1 * ep.el1 * ep.el1 * ep.el1);
+  p.ele_d2max = (float)(1.0 / ((double)ep.el1 * ep.el1));
+  p.hdb_cinv = (float)(1.0 / c);
   for (int i = 0; i < 6; ++i) p.move_scale[i] = move_scale[i];
 }
 
@@ -327,6 +336,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
   out.Ppad = Ppad;
   std::vector<float4> pos((size_t)n * Ppad);
   std::vector<float2> aux((size_t)n * Ppad);
+  std::vector<int> ncdc(n, 0);
   out.scls.assign((size_t)n * Ppad, -1);
   out.sseq.assign((size_t)n * Ppad, 0);
   for (int i = 0; i < n; ++i) {
@@ -337,8 +347,16 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
       const int t = pk.type[(size_t)i * pk.P + k];
       if (t < 0 || t >= kPadType) return fail(GD_E_INVALID, "protein conformation %d point %d: type %d outside [0, %d)", i, k, t, kPadType);
     }
-    std::stable_sort(idx.begin(), idx.end(),
-                     [&](int a, int b) { return pk.type[(size_t)i * pk.P + a] < pk.type[(size_t)i * pk.P + b]; });
+    // hydrophobic-contact points first (their rows are the only ones the
+    // hydrophobic term visits), each part sorted by point type
+    auto key = [&](int k) {
+      const size_t o = (size_t)i * pk.P + k;
+      return (pk.cdc[o] == 1 ? 0 : 64) + pk.type[o];
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
+    int nc = 0;
+    for (int k = 0; k < np; ++k) nc += pk.cdc[(size_t)i * pk.P + k] == 1;
+    ncdc[i] = nc;
     for (int j = 0; j < Ppad; ++j) {
       const size_t o = (size_t)i * Ppad + j;
       if (j < np) {
@@ -356,7 +374,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
     }
   }
   Arena ar;
-  const size_t o_pos = ar.put(pos), o_aux = ar.put(aux), o_c = ar.put(pk.center);
+  const size_t o_pos = ar.put(pos), o_aux = ar.put(aux), o_c = ar.put(pk.center), o_n = ar.put(ncdc);
   GD_CUDA(cudaMalloc(&out.arena, ar.off));
   GD_CUDA(cudaMemcpy(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice));
   out.bytes = ar.off;
@@ -364,6 +382,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
   out.pos = (float4 *)(b + o_pos);
   out.aux = (float2 *)(b + o_aux);
   out.center = (float *)(b + o_c);
+  out.ncdc = (int *)(b + o_n);
   return GD_OK;
 }
 
@@ -391,8 +410,11 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
       const float *x = &jd.lxyz[((size_t)i * L + s) * 3];
       lig[(size_t)i * lstride + a] = make_float4(x[0], x[1], x[2], jd.lcharge[s]);
     }
-  std::vector<int> ltype(L);
+  std::vector<int> ltype(L), lgend(L);
   for (int a = 0; a < L; ++a) ltype[a] = jd.ltype[perm[a]];
+  for (int a = L - 1; a >= 0; --a) lgend[a] = (a + 1 < L && ltype[a + 1] == ltype[a]) ? lgend[a + 1] : a + 1;
+  std::vector<int2> lgrp(L);
+  for (int a = 0; a < L; ++a) lgrp[a] = make_int2(ltype[a], lgend[a]);
 
   // KDE: only points with a ligand type can match (getLigCode returns 50 for others)
   std::vector<int> kidx;
@@ -426,6 +448,7 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   // pocket-specific potential gathered per sorted point: psp[t][seq3r] for class 2 points
   const int P = pk.Ppad;
   std::vector<float> psp((size_t)pk.nconf * kLigTypes * P, 0.f);
+  std::vector<uint32_t> pspmask((size_t)pk.nconf * P, 0u);
   for (int i = 0; i < pk.nconf; ++i)
     for (int j = 0; j < P; ++j) {
       const size_t o = (size_t)i * P + j;
@@ -434,12 +457,20 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
       if (col < 0 || col >= jd.psp_ncol)
         return fail(GD_E_INVALID, "protein point with residue serial %d outside the psp table [0, %d)", col,
                     jd.psp_ncol);
-      for (int t = 0; t < kLigTypes; ++t) psp[((size_t)i * kLigTypes + t) * P + j] = jd.psp[(size_t)t * jd.psp_ncol + col];
+      for (int t = 0; t < kLigTypes; ++t) {
+        const float v = jd.psp[(size_t)t * jd.psp_ncol + col];
+        psp[((size_t)i * kLigTypes + t) * P + j] = v;
+        if (v != 0.f) pspmask[o] |= 1u << t;
+      }
     }
 
   DevParams par;
   build_params(ep, jd.move_scale, par);
   std::vector<DevParams> parv(1, par);
+  std::vector<float2> hdbref((size_t)kLigTypes * kTabCols, make_float2(0.f, 0.f));
+  for (int lt = 0; lt < kLigTypes; ++lt)
+    for (int pt = 0; pt < kPadType; ++pt)
+      if (ep.hdb0[lt][pt] > 0.1f) hdbref[(size_t)lt * kTabCols + pt] = make_float2(ep.hdb0[lt][pt], ep.hdb1[lt][pt]);
 
   const int nrep = (int)jd.reps.size();
   std::vector<int> run_acc(nrep);
@@ -451,7 +482,8 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   }
 
   Arena ar;
-  const size_t o_par = ar.put(parv), o_lig = ar.put(lig), o_lt = ar.put(ltype), o_lc = ar.put(jd.lcenter);
+  const size_t o_par = ar.put(parv), o_lig = ar.put(lig), o_lg = ar.put(lgrp), o_lc = ar.put(jd.lcenter);
+  const size_t o_pm = ar.put(pspmask), o_hr = ar.put(hdbref);
   const size_t o_kde = ar.put(kde), o_mcs = ar.put(mcs), o_tcc = ar.put(jd.tcc), o_psp = ar.put(psp);
   const size_t o_mb = ar.put(jd.minus_beta), o_rep = ar.put(jd.reps), o_acc = ar.put(run_acc), o_st = ar.put(stats);
   size_t o_rec = 0;
@@ -471,14 +503,16 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   J.nlig = jd.nlig;
   J.lstride = lstride;
   J.lig = (const float4 *)(b + o_lig);
-  J.ltype = (const int *)(b + o_lt);
+  J.lgrp = (const int2 *)(b + o_lg);
   J.lcenter = (const float *)(b + o_lc);
   J.npoint_pad = P;
   J.nprt = pk.nconf;
   J.pos = pk.pos;
   J.aux = pk.aux;
+  J.ncdc = pk.ncdc;
   J.pcenter = pk.center;
   J.psp = (const float *)(b + o_psp);
+  J.pspmask = (const uint32_t *)(b + o_pm);
   J.nkde = (int)kidx.size();
   J.kde = (const float4 *)(b + o_kde);
   for (int t = 0; t < kLigTypes; ++t) {
@@ -491,6 +525,7 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   J.ntmp = jd.ntmp;
   J.minus_beta = (const float *)(b + o_mb);
   J.par = (const DevParams *)(b + o_par);
+  J.hdbref = (const float2 *)(b + o_hr);
   J.nrep = nrep;
   J.rep = (ReplicaMC *)(b + o_rep);
   J.run_acc = (int *)(b + o_acc);

@@ -67,6 +67,7 @@ struct DevPocket {
   float4 *pos = nullptr;             // [nconf][Ppad]
   float2 *aux = nullptr;             // [nconf][Ppad]
   float *center = nullptr;           // [nconf][3]
+  int *ncdc = nullptr;               // [nconf] hydrophobic-contact points (placed first)
   std::vector<int> scls, sseq;       // host: class and residue serial of each sorted point
   void *arena = nullptr;
   size_t bytes = 0;

@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_be
     const float4 *src = reinterpret_cast<const float4 *>(J.par);
     float4 *dst = reinterpret_cast<float4 *>(&par);
     for (int i = tid; i < (int)(sizeof(DevParams) / 16); i += kBD) dst[i] = src[i];
-    for (int a = tid; a < L; a += kBD) ltype_s[a] = J.ltype[a];
+    for (int a = tid; a < L; a += kBD) ltype_s[a] = J.lgrp[a].x;
   }
   __syncthreads();
 
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_be
                                      0.5f / 81.0f / 81.0f / 81.0f / 81.0f * d4 * d4);
             ehpc1 += (d2 <= 81.0f) ? w.x * hp : 0.0f;
             const float4 t4 = par.tab4[lt][pt];
-            const float2 t2 = par.tab2[lt][pt];
+            const float2 t2 = __ldg(J.hdbref + lt * kTabCols + pt);
             const float p1 = __fdividef(t4.x, d4 * d4 * d);
             const float p2 = __fdividef(t4.y, d4 * d2);
             const float p4 = p1 * par.lj0 * (1.0f + par.lj1 * d2) + 1.0f;
