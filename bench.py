@@ -254,7 +254,7 @@ def run_ours(args) -> None:
     barrier()
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
-    kernel_ms, mc_launches = ens.sync()
+    kernel_ms, mc_launches, all_launches = ens.sync(all_launches=True)
     t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -334,7 +334,7 @@ def run_ours(args) -> None:
             "plain_kernel": {"value": plain_value, "unit": UNIT, "speedup_batched_over_plain": value / world / plain_value},
             "cpu_baseline": cpu,
             "clocks": ck,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": all_launches,
         }
         print(json.dumps(line))
     if world > 1:

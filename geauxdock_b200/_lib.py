@@ -98,7 +98,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_create": (i, [vp, i, vp, i, vp, i, vp]),
         "gd_ensemble_create_complex": (i, [vp, i, vp, i, vp]),
         "gd_ensemble_init": (i, [vp]), "gd_ensemble_run": (i, [vp, i, i]),
-        "gd_ensemble_sync": (i, [vp, C.POINTER(C.c_double), ip]),
+        "gd_ensemble_sync": (i, [vp, C.POINTER(C.c_double), ip, ip]),
         "gd_ensemble_num_replicas": (i, [vp, i]), "gd_ensemble_replicas": (i, [vp, i, vp]),
         "gd_ensemble_stats": (i, [vp, i, vp]), "gd_ensemble_autotune": (i, [vp, i, C.c_char_p, i]),
         "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),

@@ -21,8 +21,9 @@ struct Options {
   int kernel = GD_KERNEL_BATCHED;
   int precision = GD_PREC_FP32;
   int warps = 0;  // 0: choose from occupancy
-  int kpl = 1;
+  int kpl = 2;
   int ab = 8;
+  int graph = 1;  // replay whole exchange intervals from a captured graph
 };
 Options g_opt;
 int g_ngpu = -1;
@@ -73,10 +74,19 @@ struct gd_ensemble {
   size_t smem = 0;
   int Pmax = 0, Kmax = 0, Kst = 0, lig_slots = 0;
   int step = 0;
+  // replica exchange over all jobs: pair-count prefix sums per parity
+  int *d_xoff = nullptr;
+  int xtot = 0;
+  // device copy of the step counter and the captured exchange interval
+  int *d_step = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int g_chunk = 0;
+  bool use_graph = true;
   // timing of the Monte Carlo launches
   std::vector<cudaEvent_t> ev;
   int ev_used = 0;
-  int launches = 0;
+  int launches = 0;      // Monte Carlo kernel launches (or graph replays of one)
+  int all_launches = 0;  // every kernel of this library launched on the stream
 };
 
 namespace {
@@ -139,6 +149,10 @@ int configure(gd_ensemble *e, TileConfig tc)
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
   e->tc = tc;
   e->smem = smem;
+  if (e->gexec) {
+    cudaGraphExecDestroy(e->gexec);
+    e->gexec = nullptr;
+  }
   GD_TRY(build_items(e));
   e->grid = std::max(1, std::min(e->n_items, occ * nsm));
   return GD_OK;
@@ -212,6 +226,20 @@ int finish_create(gd_ensemble *e)
   }
   e->lig_slots = (Lmax + 3) & ~3;
   GD_TRY(upload_jobs(e));
+  {
+    const size_t nj = e->jobs.size();
+    std::vector<int> xoff(2 * (nj + 1), 0);
+    for (int par = 0; par < 2; ++par)
+      for (size_t j = 0; j < nj; ++j) {
+        const DevJob &J = e->jobs[j].dj;
+        const int np = J.ntmp >= 2 ? (J.ntmp - par) / 2 : 0;
+        xoff[par * (nj + 1) + j + 1] = xoff[par * (nj + 1) + j] + J.nprt * J.nlig * np;
+      }
+    e->xtot = std::max(xoff[nj], xoff[2 * (nj + 1) - 1]);
+    GD_CUDA(cudaMalloc(&e->d_xoff, sizeof(int) * xoff.size()));
+    GD_CUDA(cudaMemcpy(e->d_xoff, xoff.data(), sizeof(int) * xoff.size(), cudaMemcpyHostToDevice));
+  }
+  GD_CUDA(cudaMalloc(&e->d_step, sizeof(int)));
   GD_CUDA(cudaMalloc(&e->d_queue, sizeof(int)));
   GD_CUDA(cudaMalloc(&e->d_err, sizeof(int)));
   GD_CUDA(cudaMemset(e->d_err, 0, sizeof(int)));
@@ -219,6 +247,7 @@ int finish_create(gd_ensemble *e)
   const Options o = opts();
   e->kernel = o.kernel;
   e->precision = o.precision;
+  e->use_graph = o.graph != 0;
   TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab};
   if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
   if (o.warps > 0) return configure(e, tc);
@@ -250,6 +279,8 @@ int check_err(gd_ensemble *e)
   return GD_OK;
 }
 
+KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_step);
+
 int launch_mc(gd_ensemble *e, int s_begin, int nsteps, int flags)
 {
   cudaEvent_t e0 = next_event(e), e1 = next_event(e);
@@ -259,41 +290,97 @@ int launch_mc(gd_ensemble *e, int s_begin, int nsteps, int flags)
     for (size_t j = 0; j < e->jobs.size(); ++j)
       GD_CUDA(launch_plain(e->d_jobs + j, e->jobs[j].dj.nrep, s_begin, nsteps, flags, e->d_err, e->st));
     e->launches += (int)e->jobs.size();
+    e->all_launches += (int)e->jobs.size();
   } else {
     GD_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
-    KArgs a{};
-    a.jobs = e->d_jobs;
-    a.items = e->d_items;
-    a.n_items = e->n_items;
-    a.queue = e->d_queue;
-    a.err = e->d_err;
-    a.s_begin = s_begin;
-    a.nsteps = nsteps;
-    a.flags = flags;
-    a.P = e->Pmax;
-    a.Kst = e->Kst;
-    a.lig_slots = e->lig_slots;
-    GD_CUDA(launch_kernel(0, e->precision, e->tc, a, e->grid, e->st));
+    GD_CUDA(launch_kernel(0, e->precision, e->tc, mc_args(e, s_begin, nsteps, flags, nullptr), e->grid, e->st));
     e->launches += 1;
+    e->all_launches += 1;
   }
   GD_CUDA(cudaEventRecord(e1, e->st));
   return GD_OK;
 }
 
-int launch_exchange_all(gd_ensemble *e, int x)
+KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_step)
 {
-  for (size_t j = 0; j < e->jobs.size(); ++j) {
-    const DevJob &J = e->jobs[j].dj;
-    if (J.ntmp < 2) continue;
-    GD_CUDA(launch_exchange(e->d_jobs + j, J.nprt * J.nlig, J.ntmp, x, e->st));
+  KArgs a{};
+  a.jobs = e->d_jobs;
+  a.items = e->d_items;
+  a.n_items = e->n_items;
+  a.queue = e->d_queue;
+  a.err = e->d_err;
+  a.s_begin = s_begin;
+  a.nsteps = nsteps;
+  a.flags = flags;
+  a.d_step = d_step;
+  a.P = e->Pmax;
+  a.Kst = e->Kst;
+  a.lig_slots = e->lig_slots;
+  return a;
+}
+
+// One exchange interval (queue reset, Monte Carlo chunk of `chunk` steps from
+// *d_step, exchange sweep, *d_step += chunk) captured once and replayed.
+int interval_graph(gd_ensemble *e, int chunk)
+{
+  if (e->gexec && e->g_chunk == chunk) return GD_OK;
+  if (e->gexec) {
+    cudaGraphExecDestroy(e->gexec);
+    e->gexec = nullptr;
   }
+  cudaGraph_t g = nullptr;
+  GD_CUDA(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st);
+  if (ce == cudaSuccess) ce = launch_kernel(0, e->precision, e->tc, mc_args(e, 0, chunk, kMcStoreAccept, e->d_step), e->grid, e->st);
+  if (ce == cudaSuccess)
+    ce = launch_exchange_all(e->d_jobs, e->d_xoff, (int)e->jobs.size(), e->xtot, 0, e->d_step, chunk, chunk, e->st);
+  if (ce == cudaSuccess) ce = launch_advance_step(e->d_step, chunk, e->st);
+  const cudaError_t ee = cudaStreamEndCapture(e->st, &g);
+  if (ce != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return fail(GD_E_CUDA, "graph capture: %s", cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+  }
+  ce = cudaGraphInstantiate(&e->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(GD_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ce));
+  e->g_chunk = chunk;
   return GD_OK;
 }
 
-// nsteps steps from e->step, cut at exchange boundaries.
+int exchange_sweep(gd_ensemble *e, int x)
+{
+  if (e->xtot <= 0) return GD_OK;
+  GD_CUDA(launch_exchange_all(e->d_jobs, e->d_xoff, (int)e->jobs.size(), e->xtot, x, nullptr, 0, 0, e->st));
+  e->all_launches += 1;
+  return GD_OK;
+}
+
+// nsteps steps from e->step, cut at exchange boundaries.  Whole exchange
+// intervals of a plain run (no records) replay the captured interval graph.
 int advance(gd_ensemble *e, int nsteps, int spx, int f_first, int f_all, int f_last)
 {
   int done = 0;
+  if (e->use_graph && e->kernel == GD_KERNEL_BATCHED && spx > 0 && f_first == 0 && f_all == 0 &&
+      f_last == kMcStoreAccept && e->step % spx == 0 && nsteps >= spx) {
+    const int n_int = nsteps / spx;
+    if (interval_graph(e, spx) == GD_OK) {
+      // a kernel argument rather than a copy from pageable memory, which
+      // could wait for the stream
+      GD_CUDA(launch_set_step(e->d_step, e->step, e->st));
+      cudaEvent_t e0 = next_event(e), e1 = next_event(e);
+      if (!e0 || !e1) return fail(GD_E_CUDA, "cudaEventCreate failed");
+      GD_CUDA(cudaEventRecord(e0, e->st));
+      for (int k = 0; k < n_int; ++k) GD_CUDA(cudaGraphLaunch(e->gexec, e->st));
+      GD_CUDA(cudaEventRecord(e1, e->st));
+      e->launches += n_int;
+      e->all_launches += 1 + 3 * n_int;
+      e->step += n_int * spx;
+      done = n_int * spx;
+    } else {
+      e->use_graph = false;   // capture unavailable: launch chunk by chunk
+    }
+  }
   while (done < nsteps) {
     int chunk = nsteps - done;
     if (spx > 0) chunk = std::min(chunk, spx - (e->step % spx));
@@ -301,7 +388,7 @@ int advance(gd_ensemble *e, int nsteps, int spx, int f_first, int f_all, int f_l
     GD_TRY(launch_mc(e, e->step, chunk, f));
     e->step += chunk;
     done += chunk;
-    if (spx > 0 && e->step % spx == 0) GD_TRY(launch_exchange_all(e, e->step / spx - 1));
+    if (spx > 0 && e->step % spx == 0) GD_TRY(exchange_sweep(e, e->step / spx - 1));
   }
   return GD_OK;
 }
@@ -317,6 +404,9 @@ void destroy(gd_ensemble *e)
   if (e->d_items) cudaFree(e->d_items);
   if (e->d_queue) cudaFree(e->d_queue);
   if (e->d_err) cudaFree(e->d_err);
+  if (e->d_xoff) cudaFree(e->d_xoff);
+  if (e->d_step) cudaFree(e->d_step);
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
   for (auto x : e->ev) cudaEventDestroy(x);
   if (e->st) cudaStreamDestroy(e->st);
   delete e;
@@ -386,6 +476,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "ab") {
     if (v != 4 && v != 8) return fail(GD_E_INVALID, "ab = %lld", v);
     g_opt.ab = (int)v;
+  } else if (n == "graph") {
+    if (v != 0 && v != 1) return fail(GD_E_INVALID, "graph = %lld", v);
+    g_opt.graph = (int)v;
   } else {
     return fail(GD_E_INVALID, "unknown option '%s'", name);
   }
@@ -402,6 +495,7 @@ long long gd_get_option(const char *name)
   if (n == "warps") return g_opt.warps;
   if (n == "kpl") return g_opt.kpl;
   if (n == "ab") return g_opt.ab;
+  if (n == "graph") return g_opt.graph;
   return GD_E_INVALID;
 }
 
@@ -818,7 +912,7 @@ int gd_ensemble_run(gd_ensemble_t *e, int nsteps, int steps_per_exchange)
   return advance(e, nsteps, steps_per_exchange, 0, 0, kMcStoreAccept);
 }
 
-int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches)
+int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches, int *all_launches)
 {
   if (!e) return fail(GD_E_INVALID, "null ensemble");
   GD_TRY(set_device(e->device));
@@ -831,8 +925,10 @@ int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches)
   }
   if (kernel_ms) *kernel_ms = ms;
   if (launches) *launches = e->launches;
+  if (all_launches) *all_launches = e->all_launches;
   e->ev_used = 0;
   e->launches = 0;
+  e->all_launches = 0;
   return check_err(e);
 }
 
@@ -949,6 +1045,7 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   for (void *p : snaps) cudaFree(p);
   e->ev_used = 0;
   e->launches = 0;
+  e->all_launches = 0;
   if (rc == GD_OK) rc = configure(e, best);
   char line[160];
   snprintf(line, sizeof line, "chosen: warps=%d kpl=%d ab=%d\n", best.warps_per_cta, best.kpl, best.ab);

@@ -157,6 +157,7 @@ struct KArgs {
   int *queue;
   int *err;
   int s_begin, nsteps, flags;
+  const int *d_step;       // if set, steps start at *d_step + s_begin (graph replay)
   int P, Kst, lig_slots;   // smem layout parameters (maximum over the launched jobs)
   // pose evaluation
   const int *conf;
@@ -179,6 +180,15 @@ cudaError_t launch_kernel(int mode, int precision, const TileConfig &tc, const K
 // Pose evaluation reading the packed job from global memory (8 poses per 256-thread CTA, grid-stride).
 cudaError_t launch_eval_global(int precision, const DevJob *d_job, const int *conf, const float *mm, int n,
                                float *out, float *raw, int *err, int grid, cudaStream_t st);
+
+// Replica-exchange sweep over all jobs (d_xoff: [2][njob+1] pair-count prefix sums per
+// parity; total: the larger of the two totals).  With d_step, the sweep index is
+// (*d_step + chunk) / spx - 1, else x.
+cudaError_t launch_exchange_all(const DevJob *d_jobs, const int *d_xoff, int njob, int total, int x,
+                                const int *d_step, int spx, int chunk, cudaStream_t st);
+// *d_step += n on the stream.
+cudaError_t launch_set_step(int *d_step, int v, cudaStream_t st);
+cudaError_t launch_advance_step(int *d_step, int n, cudaStream_t st);
 
 // Replica-exchange sweep x of one job (ngroup = nprt * nlig groups of ntmp temperatures).
 cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cudaStream_t st);

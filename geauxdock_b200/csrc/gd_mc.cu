@@ -595,7 +595,8 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         }
         const bool initial = (A.flags & kMcInitial) != 0;
 
-        for (int s = A.s_begin; s < A.s_begin + A.nsteps; ++s) {
+        const int s0 = A.d_step ? *A.d_step + A.s_begin : A.s_begin;
+        for (int s = s0; s < s0 + A.nsteps; ++s) {
           if (acc) {
             // record the old state, kernel_cuda_l1_montecarlo.cu:290-297
             if (lane == 0) srep->step = s;
@@ -677,15 +678,14 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
 // Replica exchange between adjacent temperatures.  Sweep x pairs (t, t+1) for
 // t = x mod 2, x mod 2 + 2, ... in every (protein conf p, ligand conf l)
 // group; replica index n_tmp*n_lig*p + n_lig*t + l (src/frontend/util.C:380).
-__global__ void exchange_kernel(const DevJob *jobp, int x)
+// Pair k of the sweep of job J:
+__device__ void exchange_one(const DevJob &J, int x, int k)
 {
-  const DevJob &J = *jobp;
   const int npair = (J.ntmp - (x & 1)) / 2;
   if (npair <= 0) return;
   const int ngroup = J.nprt * J.nlig;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= ngroup * npair) return;
-  const int g = tid / npair, i = tid % npair;
+  if (k >= ngroup * npair) return;
+  const int g = k / npair, i = k % npair;
   const int p = g / J.nlig, l = g % J.nlig;
   const int t = (x & 1) + 2 * i;
   const int ga = J.ntmp * J.nlig * p + J.nlig * t + l;
@@ -701,16 +701,16 @@ __global__ void exchange_kernel(const DevJob *jobp, int x)
   J.stats[rb].n_exch_try += 1;
   if (log(u) < lr) {
 #pragma unroll
-    for (int k = 0; k < 10; ++k) {
-      const float tmp = A->energy[k];
-      A->energy[k] = B->energy[k];
-      B->energy[k] = tmp;
+    for (int q = 0; q < 10; ++q) {
+      const float tmp = A->energy[q];
+      A->energy[q] = B->energy[q];
+      B->energy[q] = tmp;
     }
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const float tmp = A->movematrix[k];
-      A->movematrix[k] = B->movematrix[k];
-      B->movematrix[k] = tmp;
+    for (int q = 0; q < 6; ++q) {
+      const float tmp = A->movematrix[q];
+      A->movematrix[q] = B->movematrix[q];
+      B->movematrix[q] = tmp;
     }
     J.run_acc[ra] = 1;
     J.run_acc[rb] = 1;
@@ -718,6 +718,33 @@ __global__ void exchange_kernel(const DevJob *jobp, int x)
     J.stats[rb].n_exch_acc += 1;
   }
 }
+
+__global__ void exchange_kernel(const DevJob *jobp, int x)
+{
+  exchange_one(*jobp, x, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// One sweep over every job of an ensemble.  xoff[parity][j] is the prefix sum
+// of the pair counts (groups x pairs of that parity).  The sweep index is x, or
+// with d_step the sweep that ends the chunk [*d_step, *d_step + chunk).
+__global__ void exchange_all_kernel(const DevJob *jobs, const int *xoff, int njob, int x, const int *d_step,
+                                    int spx, int chunk)
+{
+  if (d_step) x = (*d_step + chunk) / spx - 1;
+  const int *off = xoff + (x & 1) * (njob + 1);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= off[njob]) return;
+  int lo = 0, hi = njob;  // off[lo] <= tid < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= tid) lo = mid;
+    else hi = mid;
+  }
+  exchange_one(jobs[lo], x, tid - off[lo]);
+}
+
+__global__ void advance_step_kernel(int *d_step, int n) { *d_step += n; }
+__global__ void set_step_kernel(int *d_step, int v) { *d_step = v; }
 
 // Pose evaluation that reads the packed job straight from global memory (no
 // shared-memory staging, no work items): warp w of the grid evaluates poses
@@ -826,6 +853,26 @@ int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem)
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, tc.warps_per_cta * 32, smem) != cudaSuccess) return 0;
   return nb;
+}
+
+cudaError_t launch_exchange_all(const DevJob *d_jobs, const int *d_xoff, int njob, int total, int x,
+                                const int *d_step, int spx, int chunk, cudaStream_t st)
+{
+  if (total <= 0) return cudaSuccess;
+  exchange_all_kernel<<<(total + 255) / 256, 256, 0, st>>>(d_jobs, d_xoff, njob, x, d_step, spx, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_step(int *d_step, int v, cudaStream_t st)
+{
+  set_step_kernel<<<1, 1, 0, st>>>(d_step, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance_step(int *d_step, int n, cudaStream_t st)
+{
+  advance_step_kernel<<<1, 1, 0, st>>>(d_step, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cudaStream_t st)

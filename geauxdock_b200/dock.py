@@ -121,11 +121,13 @@ class Ensemble:
     def run(self, nsteps: int, steps_per_exchange: int = 0) -> None:
         check(self.lib.gd_ensemble_run(self.h, nsteps, steps_per_exchange))
 
-    def sync(self):
+    def sync(self, all_launches: bool = False):
+        """Wait; returns (Monte Carlo kernel ms, Monte Carlo launches[, all kernel launches])."""
         ms = C.c_double()
         nl = C.c_int()
-        check(self.lib.gd_ensemble_sync(self.h, C.byref(ms), C.byref(nl)))
-        return ms.value, nl.value
+        na = C.c_int()
+        check(self.lib.gd_ensemble_sync(self.h, C.byref(ms), C.byref(nl), C.byref(na)))
+        return (ms.value, nl.value, na.value) if all_launches else (ms.value, nl.value)
 
     def replicas(self, job: int = 0) -> np.ndarray:
         n = check(self.lib.gd_ensemble_num_replicas(self.h, job))

@@ -88,8 +88,10 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
 #define GD_PREC_FP64 2        /* FP64 pair energies                               */
 
 /* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*), "warps" (replicas
- * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape).  Applies to objects
- * created afterwards on the calling process. */
+ * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape; default 2, 8),
+ * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
+ * 0: launch them one by one).  Applies to objects created afterwards on the
+ * calling process. */
 int gd_set_option(const char *name, long long value);
 long long gd_get_option(const char *name);
 
@@ -175,11 +177,15 @@ int gd_ensemble_create_complex(const Complex *const *cx, int n, const uint64_t *
 /* Initial energies (no move, forced accept). */
 int gd_ensemble_init(gd_ensemble_t *e);
 /* Advance every replica by nsteps MC steps, with a replica-exchange sweep
- * every steps_per_exchange steps (0 = none).  Asynchronous. */
+ * every steps_per_exchange steps (0 = none).  Asynchronous.  Whole exchange
+ * intervals are replayed from one captured CUDA graph (Monte Carlo chunk,
+ * exchange sweep, step counter). */
 int gd_ensemble_run(gd_ensemble_t *e, int nsteps, int steps_per_exchange);
-/* Wait for the device; kernel_ms: device time of the MC kernels since the
- * last call (CUDA events on the ensemble's stream), launches: their count. */
-int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches);
+/* Wait for the device; kernel_ms: device time of the Monte Carlo launches
+ * since the last call (CUDA events on the ensemble's stream; a replayed
+ * exchange interval counts as one launch), launches: their count,
+ * all_launches: every kernel of the library launched on the stream. */
+int gd_ensemble_sync(gd_ensemble_t *e, double *kernel_ms, int *launches, int *all_launches);
 int gd_ensemble_num_replicas(const gd_ensemble_t *e, int job);
 int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out);
 /* Per replica: {n_steps, n_accept, n_exch_try, n_exch_acc, mean E, var E, best E, best step}. */

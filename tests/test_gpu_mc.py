@@ -181,3 +181,34 @@ def test_invalid_inputs_rejected(lib, enepara):
     bad[0]["mcs"][0]["x"][:] = Lo.MCS_INVALID_COORD   # an MCS row with no coordinate
     with pytest.raises(GdockError):
         dock.Ensemble.from_complexes([bad], [1])
+
+
+def test_graph_replay_matches_launches(lib, enepara, oracle_lib):
+    """Whole exchange intervals replayed from the captured graph (one exchange
+    launch over every job, device step counter) leave the same bytes as
+    chunk-by-chunk launches, for jobs with different ladders and a remainder
+    chunk; each job still follows its own oracle chain."""
+    cxs = [_small_ensemble(enepara, seed=41, L=14, temps=(0.3, 0.9, 2.7)),
+           _small_ensemble(enepara, seed=42, L=30, P=420, nlig=2, temps=(0.2, 0.4, 0.8, 1.6, 3.2)),
+           _small_ensemble(enepara, seed=43, L=9, nprt=1, nlig=1, temps=(1.0,))]
+    seeds = [5, 6, 7]
+    out = {}
+    try:
+        for graph in (1, 0):
+            check(lib.gd_set_option(b"graph", graph))
+            with dock.Ensemble.from_complexes(cxs, seeds) as ens:
+                ens.init()
+                ens.run(130, 20)
+                ens.run(40, 20)
+                _, _, nall = ens.sync(all_launches=True)
+                out[graph] = [(ens.replicas(j).tobytes(), ens.stats(j).tobytes()) for j in range(3)]
+                assert nall > 0
+    finally:
+        check(lib.gd_set_option(b"graph", 1))
+    assert out[1] == out[0]
+    for j, cx in enumerate(cxs):
+        ref = _oracle_run(oracle_lib, cx, seeds[j], 170, spx=20)
+        n = int(cx[0]["size"]["n_rep"])
+        got = np.frombuffer(out[1][j][0], dtype=Lo.REPLICA)
+        same = _same_trajectory(got, ref[0]["replica"][:n])
+        assert same.mean() >= 0.9, (j, same.mean())

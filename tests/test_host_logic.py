@@ -64,9 +64,13 @@ def test_options_validated(lib):
         check(lib.gd_set_option(b"kernel", 7))
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"nonsense", 1))
+    assert lib.gd_get_option(b"kpl") == 2          # default pair-tile shape
+    check(lib.gd_set_option(b"kpl", 4))
+    assert lib.gd_get_option(b"kpl") == 4
     check(lib.gd_set_option(b"kpl", 2))
-    assert lib.gd_get_option(b"kpl") == 2
-    check(lib.gd_set_option(b"kpl", 1))
+    assert lib.gd_get_option(b"graph") == 1
+    with pytest.raises(GdockError):
+        check(lib.gd_set_option(b"graph", 2))
 
 
 def test_eval_rejects_bad_conformation_before_device_work(lib, enepara):
