@@ -61,7 +61,17 @@ def _args():
                    help="MC steps per bench step (= steps between exchange sweeps)")
     p.add_argument("--tile", default="", help="warps,kpl,ab: fixed tile shape (skips the autotuner)")
     p.add_argument("--skip-extras", action="store_true",
-                   help="only the timed batched kernel (for profiling): no plain kernel, e2e or CPU baseline")
+                   help="only the timed batched kernel (for profiling): no plain kernel, e2e, CPU baseline, "
+                        "screening or serving legs")
+    p.add_argument("--workload", choices=["all", "ensemble", "screening", "serving"], default="all",
+                   help="ensemble: the headline line only; screening / serving: that leg alone")
+    p.add_argument("--screen-ligands", type=int, default=512)
+    p.add_argument("--screen-intervals", type=int, default=2)
+    p.add_argument("--plain-ligands", type=int, default=48,
+                   help="ligands of the screening set timed with the plain one-launch-per-ligand kernel")
+    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
+    p.add_argument("--serve-steps", type=int, default=2000)
     return p.parse_args()
 
 
@@ -197,6 +207,164 @@ def run_reference(args) -> None:
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def _pct(x, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
+
+
+def run_screening(args, local: int) -> dict:
+    """Batched uneven screening: ligands of U[12, 64] atoms x 10 conformations x
+    5 protein conformations x 8 temperatures against one 2000-point pocket, all
+    ligands in one persistent launch per exchange interval (replayed from a CUDA
+    graph), against the plain kernel launched once per ligand."""
+    import torch
+
+    from geauxdock_b200 import dock, params, synth
+    from geauxdock_b200._lib import check, load
+
+    lib = load()
+    ep = params.optimize_enepara(params.default_enepara0())
+    pk, jobs = synth.config3(seed=1, nligand=args.screen_ligands)
+    n_rep = sum(j.nlig * j.ntmp * pk.nconf for j in jobs)
+    spi = STEPS_PER_INTERVAL
+    check(lib.gd_set_option(b"kernel", 0))
+    t0 = time.perf_counter()
+    ens = dock.Ensemble.from_jobs([pk], jobs, ep, device=local)
+    pack_s = time.perf_counter() - t0
+    ens.init()
+    ens.sync()
+    tune = "" if args.no_autotune else ens.autotune(2)
+    ens.run(spi, spi)                    # warm-up: captures the interval graph
+    ens.sync()
+    stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.screen_intervals):
+        ens.run(spi, spi)
+    b.record(stream)
+    b.synchronize()
+    _, mc_launches, all_launches = ens.sync(all_launches=True)
+    batched = n_rep * spi * args.screen_intervals / (a.elapsed_time(b) / 1e3)
+    ens.close()
+
+    # plain kernel, one launch per ligand per interval, on the first ligands
+    sub = jobs[:args.plain_ligands]
+    n_sub = sum(j.nlig * j.ntmp * pk.nconf for j in sub)
+    check(lib.gd_set_option(b"kernel", 1))
+    plain = dock.Ensemble.from_jobs([pk], sub, ep, device=local)
+    plain.init()
+    plain.run(spi, spi)
+    plain.sync()
+    pstream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(plain.h), device=torch.device("cuda", local))
+    a.record(pstream)
+    plain.run(spi, spi)
+    b.record(pstream)
+    b.synchronize()
+    _, plain_launches = plain.sync()
+    plain_value = n_sub * spi / (a.elapsed_time(b) / 1e3)
+    plain.close()
+    check(lib.gd_set_option(b"kernel", 0))
+    return {"workload": f"{args.screen_ligands} ligands of U[12,64] atoms x 10 conformations, 1 pocket of 2000 "
+                        "points x 5 conformations, 600 KDE points, 16 MCS templates, 8 temperatures 0.3-3.0",
+            "replicas": n_rep, "value": batched, "unit": UNIT,
+            "timed": f"{args.screen_intervals} exchange intervals of {spi} MC steps (device time)",
+            "launches": {"mc": mc_launches, "all": all_launches}, "pack_s": pack_s,
+            "autotune": tune.strip().splitlines()[-1] if tune else "off",
+            "plain_one_launch_per_ligand": {"value": plain_value, "unit": UNIT, "ligands": len(sub),
+                                            "launches": plain_launches},
+            "speedup_over_plain": batched / plain_value}
+
+
+def pe_n(job, pockets) -> int:
+    return job.nlig * job.ntmp * pockets[job.pocket].nconf
+
+
+def run_serving(args, local: int) -> dict:
+    """Serving: Poisson arrivals of docking requests (ligands log-uniform in
+    [8, 80] atoms, 10 x 5 x 8 replicas, 2000 MC steps) against 4 resident
+    pockets of 800, 1500, 2200 and 3000 points, admitted by a 100 GB HBM
+    budget.  Latency = completion - submission on the server's clock."""
+    import numpy as np
+
+    from geauxdock_b200 import dock, params, synth
+    from geauxdock_b200._lib import check, load
+
+    lib = load()
+    check(lib.gd_set_option(b"kernel", 0))
+    ep = params.optimize_enepara(params.default_enepara0())
+    pockets = synth.serving_pockets(seed=1)
+    rng = np.random.default_rng(7)
+    n = args.serve_requests
+    jobs = [synth.serving_job(rng, pockets, seed=50_000 + i) for i in range(2 * n + 2)]
+    steps = args.serve_steps
+
+    def stream(srv, batch, rate, seed):
+        arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, len(batch)))
+        t0 = time.perf_counter()
+        for j, t in zip(batch, arr):
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            srv.submit(j, steps, STEPS_PER_INTERVAL, results=False)
+        srv.drain(-1)
+        res = srv.poll(len(batch), 0)
+        assert len(res) == len(batch) and all(r["status"] == 0 for r in res), res[:2]
+        lat = [r["t_done"] - r["t_submit"] for r in res]
+        span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+        evals = sum(r["nrep"] * (r["steps"] + 1) for r in res)
+        return {"rate_req_s": rate, "requests": len(batch), "p50_s": _pct(lat, 50), "p99_s": _pct(lat, 99),
+                "mean_queue_s": float(np.mean([r["t_admit"] - r["t_submit"] for r in res])),
+                "value": evals / span, "unit": UNIT, "req_per_s": len(batch) / span, "span_s": span}
+
+    with dock.Server(pockets, ep, device=local, max_atoms=80) as srv:
+        srv.submit(jobs[-1], 100, STEPS_PER_INTERVAL, results=False)   # warm-up
+        srv.submit(jobs[-2], 100, STEPS_PER_INTERVAL, results=False)
+        srv.drain(-1)
+        srv.poll(4, 0)
+        s0 = srv.stats()
+        named = stream(srv, jobs[:n], args.serve_rate, 11)
+        s1 = srv.stats()
+        # below capacity: 70% of the request rate the saturated run sustained
+        light_rate = 0.7 * named["req_per_s"]
+        light = stream(srv, jobs[n:n + max(8, n // 2)], light_rate, 12)
+        s2 = srv.stats()
+    # plain kernel, one request at a time (one launch per request per interval), a few requests
+    import torch
+
+    check(lib.gd_set_option(b"kernel", 1))
+    p_evals, p_ms = 0, 0.0
+    for j in jobs[:3]:
+        pe = dock.Ensemble.from_jobs(pockets, [j], ep, device=local)
+        pe.init()
+        pe.sync()
+        st_ = torch.cuda.ExternalStream(lib.gd_ensemble_stream(pe.h), device=torch.device("cuda", local))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st_)
+        pe.run(4 * STEPS_PER_INTERVAL, STEPS_PER_INTERVAL)
+        b.record(st_)
+        b.synchronize()
+        pe.sync()
+        p_ms += a.elapsed_time(b)
+        p_evals += pe_n(j, pockets) * 4 * STEPS_PER_INTERVAL
+        pe.close()
+    check(lib.gd_set_option(b"kernel", 0))
+    plain = {"value": p_evals / (p_ms / 1e3), "unit": UNIT,
+             "sample": f"first 3 requests one at a time, {4 * STEPS_PER_INTERVAL} MC steps each (device time)"}
+    dev_s = (s1["device_ms"] - s0["device_ms"]) / 1e3
+    named["gpu_busy_frac"] = dev_s / named["span_s"]
+    light["gpu_busy_frac"] = (s2["device_ms"] - s1["device_ms"]) / 1e3 / light["span_s"]
+    return {"workload": f"Poisson arrivals, ligands log-uniform [8,80] atoms, 10x5x8 replicas, {steps} MC steps, "
+                        "exchange every 50, 4 resident pockets (800/1500/2200/3000 points x 5), 100 GB HBM budget",
+            "named_rate": named, "below_capacity": light, "plain_one_launch_per_request": plain,
+            "speedup_over_plain": named["value"] / plain["value"],
+            "server": {"warps_per_cta": s2["warps_per_cta"], "grid": s2["grid"],
+                       "max_active_replicas": s2["max_active_replicas"], "rounds": s2["rounds"],
+                       "launches": s2["launches"], "peak_bytes": s2["peak_bytes"]},
+            "sample": f"{named['requests']} + {light['requests']} requests (the named stream has 10000; "
+                      "bounded so the bench ends in minutes)"}
+
+
 def run_ours(args) -> None:
     import ctypes as C
 
@@ -206,6 +374,11 @@ def run_ours(args) -> None:
 
     rank, world, local = _dist()
     torch.cuda.set_device(local)
+    if args.workload in ("screening", "serving"):
+        if rank == 0:
+            leg = run_screening(args, local) if args.workload == "screening" else run_serving(args, local)
+            print(json.dumps({"metric": METRIC, "workload": args.workload, **leg}))
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
@@ -313,6 +486,11 @@ def run_ours(args) -> None:
     e2e_steps = int(cx[0]["mcpara"]["steps_total"])
     e2e_value = world * n_rep * e2e_steps / e2e_s
 
+    screening = serving = None
+    if world == 1 and args.workload == "all":
+        screening = run_screening(args, local)
+        serving = run_serving(args, local)
+
     if rank == 0:
         cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "skipped (--no-cpu-baseline)"}
         if not args.no_cpu_baseline and world == 1:
@@ -336,6 +514,9 @@ def run_ours(args) -> None:
             "clocks": ck,
             "gpu_launches": all_launches,
         }
+        if screening is not None:
+            line["screening"] = screening
+            line["serving"] = serving
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -41,7 +41,45 @@ EXPORTED = [
     "gd_ensemble_autotune", "gd_ensemble_destroy",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
     "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
+    "gd_server_config_default", "gd_server_create", "gd_server_submit", "gd_server_poll", "gd_server_drain",
+    "gd_server_get_stats", "gd_server_destroy",
 ]
+
+
+class ServerConfig(C.Structure):
+    """gd_server_config_t."""
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_ulonglong), ("max_active_replicas", C.c_int), ("max_jobs", C.c_int),
+        ("max_replicas_per_job", C.c_int), ("max_atoms", C.c_int), ("steps_per_round", C.c_int),
+        ("kde_stage", C.c_int), ("warps", C.c_int), ("device", C.c_int),
+    ]
+
+
+class Request(C.Structure):
+    """gd_request_t."""
+    _fields_ = [
+        ("job", C.c_void_p), ("steps", C.c_int), ("steps_per_exchange", C.c_int),
+        ("replicas_out", C.c_void_p), ("stats_out", C.c_void_p),
+    ]
+
+
+class Result(C.Structure):
+    """gd_result_t."""
+    _fields_ = [
+        ("ticket", C.c_longlong), ("status", C.c_int), ("nrep", C.c_int), ("steps", C.c_int), ("pad_", C.c_int),
+        ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    """gd_server_stats_t."""
+    _fields_ = [
+        ("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+        ("queued", C.c_longlong), ("outstanding", C.c_longlong), ("rounds", C.c_longlong),
+        ("launches", C.c_longlong), ("pose_evals", C.c_double), ("device_ms", C.c_double), ("now", C.c_double),
+        ("used_bytes", C.c_ulonglong), ("peak_bytes", C.c_ulonglong),
+        ("warps_per_cta", C.c_int), ("grid", C.c_int), ("max_active_replicas", C.c_int), ("pad_", C.c_int),
+    ]
 
 
 class GdockError(RuntimeError):
@@ -105,6 +143,13 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),
         "gd_eval_poses_noalloc": (i, [vp, i, vp, vp, i, vp, vp, vp]), "gd_noalloc_scratch_bytes": (C.c_size_t, []),
+        "gd_server_config_default": (None, [vp]),
+        "gd_server_create": (i, [vp, i, vp, vp, vp]),
+        "gd_server_submit": (i, [vp, vp, C.POINTER(ll)]),
+        "gd_server_poll": (i, [vp, vp, i, i]),
+        "gd_server_drain": (i, [vp, i]),
+        "gd_server_get_stats": (i, [vp, vp]),
+        "gd_server_destroy": (i, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1101,6 +1101,14 @@ extern "C" long long gd_layout(const char *what)
   GD_L("EnePara.hpl0", offsetof(EnePara, hpl0))
   GD_L("EnePara.kde2", offsetof(EnePara, kde2))
   GD_L("Record.next_entry", offsetof(Record, next_entry))
+  GD_L("sizeof.gd_job_desc_t", sizeof(gd_job_desc_t))
+  GD_L("sizeof.gd_pocket_desc_t", sizeof(gd_pocket_desc_t))
+  GD_L("sizeof.gd_server_config_t", sizeof(gd_server_config_t))
+  GD_L("sizeof.gd_request_t", sizeof(gd_request_t))
+  GD_L("sizeof.gd_result_t", sizeof(gd_result_t))
+  GD_L("sizeof.gd_server_stats_t", sizeof(gd_server_stats_t))
+  GD_L("gd_server_stats_t.warps_per_cta", offsetof(gd_server_stats_t, warps_per_cta))
+  GD_L("gd_result_t.t_done", offsetof(gd_result_t, t_done))
 #undef GD_L
   return -1;
 }

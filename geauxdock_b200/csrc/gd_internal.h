@@ -116,6 +116,11 @@ struct DevJob {
   uint32_t key0, key1;     // Philox key (job seed)
   int rid_base;            // global index of local replica 0 (Philox counter, exchange partners)
   int nrep_total;          // replicas of the whole ensemble (nlig * nprt * ntmp)
+  // per-job scheduling state (zero for ensembles; set each round by the server)
+  int step0;               // added to the launch's first step: the job's own step count
+  int nsteps;              // > 0: steps this job runs in a launch (<= the launch's), else the launch's
+  int xsweep;              // exchange sweep run for this job by exchange_jobs_kernel (< 0: none)
+  int pad_;
 };
 
 // One unit of work of the batched kernel: `count` consecutive replicas of
@@ -188,6 +193,9 @@ cudaError_t launch_exchange_all(const DevJob *d_jobs, const int *d_xoff, int njo
                                 const int *d_step, int spx, int chunk, cudaStream_t st);
 // *d_step += n on the stream.
 cudaError_t launch_set_step(int *d_step, int v, cudaStream_t st);
+// One exchange sweep per job, sweep index jobs[j].xsweep (skipped when < 0);
+// max_pairs bounds groups x pairs over the jobs.
+cudaError_t launch_exchange_jobs(const DevJob *d_jobs, int njob, int max_pairs, cudaStream_t st);
 cudaError_t launch_advance_step(int *d_step, int n, cudaStream_t st);
 
 // Replica-exchange sweep x of one job (ngroup = nprt * nlig groups of ntmp temperatures).

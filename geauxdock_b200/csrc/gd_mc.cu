@@ -595,8 +595,9 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         }
         const bool initial = (A.flags & kMcInitial) != 0;
 
-        const int s0 = A.d_step ? *A.d_step + A.s_begin : A.s_begin;
-        for (int s = s0; s < s0 + A.nsteps; ++s) {
+        const int s0 = (A.d_step ? *A.d_step + A.s_begin : A.s_begin) + J.step0;
+        const int nsteps = J.nsteps > 0 ? min(J.nsteps, A.nsteps) : A.nsteps;
+        for (int s = s0; s < s0 + nsteps; ++s) {
           if (acc) {
             // record the old state, kernel_cuda_l1_montecarlo.cu:290-297
             if (lane == 0) srep->step = s;
@@ -661,7 +662,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
           RepStats &S = J.stats[r];
           S.e_sum += wst->e_sum;
           S.e_sum2 += wst->e_sum2;
-          S.n_steps += A.nsteps;
+          S.n_steps += nsteps;
           S.n_accept += wst->n_acc;
           S.best_e = wst->best_e;
           S.best_step = wst->best_step;
@@ -741,6 +742,15 @@ __global__ void exchange_all_kernel(const DevJob *jobs, const int *xoff, int njo
     else hi = mid;
   }
   exchange_one(jobs[lo], x, tid - off[lo]);
+}
+
+// One sweep per job with the job's own sweep index (jobs admitted at
+// different times are at different steps): blockIdx.y is the job.
+__global__ void exchange_jobs_kernel(const DevJob *jobs)
+{
+  const DevJob &J = jobs[blockIdx.y];
+  if (J.xsweep < 0) return;
+  exchange_one(J, J.xsweep, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void advance_step_kernel(int *d_step, int n) { *d_step += n; }
@@ -860,6 +870,13 @@ cudaError_t launch_exchange_all(const DevJob *d_jobs, const int *d_xoff, int njo
 {
   if (total <= 0) return cudaSuccess;
   exchange_all_kernel<<<(total + 255) / 256, 256, 0, st>>>(d_jobs, d_xoff, njob, x, d_step, spx, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_exchange_jobs(const DevJob *d_jobs, int njob, int max_pairs, cudaStream_t st)
+{
+  if (njob <= 0 || max_pairs <= 0) return cudaSuccess;
+  exchange_jobs_kernel<<<dim3((max_pairs + 127) / 128, njob), 128, 0, st>>>(d_jobs);
   return cudaGetLastError();
 }
 

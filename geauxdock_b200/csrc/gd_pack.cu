@@ -386,8 +386,9 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
   return GD_OK;
 }
 
-int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
-             DevJobBuf &out)
+namespace {
+int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
+                  cudaStream_t st, bool async, DevJobBuf &out)
 {
   out = DevJobBuf{};
   const int L = jd.L;
@@ -490,9 +491,16 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   const bool alloc_rec = want_records && rec == nullptr;
   if (alloc_rec) o_rec = ar.take(sizeof(Record) * (size_t)nrep);
 
-  GD_CUDA(cudaMalloc(&out.arena, ar.off));
-  if (alloc_rec) GD_CUDA(cudaMemset(out.arena, 0, ar.off));
-  GD_CUDA(cudaMemcpy(out.arena, ar.host.data(), alloc_rec ? o_rec : ar.off, cudaMemcpyHostToDevice));
+  if (async) {
+    // stream-ordered: no device-wide synchronisation (a pageable copy may wait for `st` only)
+    GD_CUDA(cudaMallocAsync(&out.arena, ar.off, st));
+    if (alloc_rec) GD_CUDA(cudaMemsetAsync(out.arena, 0, ar.off, st));
+    GD_CUDA(cudaMemcpyAsync(out.arena, ar.host.data(), alloc_rec ? o_rec : ar.off, cudaMemcpyHostToDevice, st));
+  } else {
+    GD_CUDA(cudaMalloc(&out.arena, ar.off));
+    if (alloc_rec) GD_CUDA(cudaMemset(out.arena, 0, ar.off));
+    GD_CUDA(cudaMemcpy(out.arena, ar.host.data(), alloc_rec ? o_rec : ar.off, cudaMemcpyHostToDevice));
+  }
   out.bytes = ar.off;
   out.own_rec = alloc_rec;
   unsigned char *b = (unsigned char *)out.arena;
@@ -535,13 +543,32 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
   J.key1 = (uint32_t)(jd.seed >> 32);
   J.rid_base = jd.rid_base;
   J.nrep_total = jd.nrep_total;
+  J.xsweep = -1;
   return GD_OK;
+}
+}  // namespace
+
+int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
+             DevJobBuf &out)
+{
+  return pack_job_impl(jd, pk, ep, want_records, rec, nullptr, false, out);
+}
+
+int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cudaStream_t st, DevJobBuf &out)
+{
+  return pack_job_impl(jd, pk, ep, false, nullptr, st, true, out);
 }
 
 void free_pocket(DevPocket &p)
 {
   if (p.arena) cudaFree(p.arena);
   p = DevPocket{};
+}
+
+void free_job_async(DevJobBuf &j, cudaStream_t st)
+{
+  if (j.arena) cudaFreeAsync(j.arena, st);
+  j = DevJobBuf{};
 }
 
 void free_job(DevJobBuf &j)

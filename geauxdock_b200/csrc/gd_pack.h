@@ -96,7 +96,10 @@ int pack_pocket(const PocketData &pk, DevPocket &out);
 // rec: external device Record array (nullptr with want_records allocates one).
 int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
              DevJobBuf &out);
+// Stream-ordered variant (cudaMallocAsync + a copy on `st`), no records.
+int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cudaStream_t st, DevJobBuf &out);
 void free_pocket(DevPocket &p);
 void free_job(DevJobBuf &j);
+void free_job_async(DevJobBuf &j, cudaStream_t st);
 
 }  // namespace gd

@@ -156,3 +156,92 @@ class Ensemble:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Server:
+    """A request loop on one GPU (gd_server_*): resident pockets, requests
+    admitted by an HBM budget into running rounds (continuous batching)."""
+
+    def __init__(self, pockets, enepara: np.ndarray, device: int = 0, **config):
+        from . import synth
+        from ._lib import PocketDesc, ServerConfig
+
+        self.lib = load()
+        self.h = None
+        self._keep: list = []
+        cfg = ServerConfig()
+        self.lib.gd_server_config_default(C.byref(cfg))
+        for k, v in config.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown server option {k!r}")
+            setattr(cfg, k, v)
+        cfg.device = device
+        parr = (PocketDesc * len(pockets))(*[synth.pocket_desc(p, self._keep) for p in pockets])
+        ep = np.array([enepara], dtype=Lo.ENEPARA)
+        self._keep.append(ep)
+        h = C.c_void_p()
+        check(self.lib.gd_server_create(parr, len(pockets), C.c_void_p(ep.ctypes.data), C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._pocket_nconf = [p.nconf for p in pockets]
+        self._live: dict = {}   # ticket -> (arrays kept alive, replicas, stats)
+
+    def submit(self, job, steps: int, steps_per_exchange: int = 0, results: bool = True) -> int:
+        """Queue a docking request (synth.Job-like; job.pocket indexes the pockets); returns its ticket."""
+        from . import synth
+        from ._lib import Request
+
+        keep: list = []
+        jd = synth.job_desc(job, keep)
+        keep.append(jd)
+        nrep = job.nlig * job.ntmp * self._nconf(job.pocket)
+        rep = Lo.aligned_zeros(Lo.REPLICA, nrep) if results else None
+        st = np.zeros((nrep, 8), np.float64) if results else None
+        req = Request()
+        req.job = C.addressof(jd)
+        req.steps = steps
+        req.steps_per_exchange = steps_per_exchange
+        req.replicas_out = rep.ctypes.data if results else None
+        req.stats_out = st.ctypes.data if results else None
+        t = C.c_longlong()
+        check(self.lib.gd_server_submit(self.h, C.byref(req), C.byref(t)))
+        self._live[t.value] = (keep, rep, st)
+        return t.value
+
+    def _nconf(self, pocket: int) -> int:
+        return self._pocket_nconf[pocket]
+
+    def poll(self, max_results: int = 64, timeout_ms: int = -1) -> list:
+        """Finished requests: dicts with ticket, status, times and (if kept) replicas / stats."""
+        from ._lib import Result
+
+        buf = (Result * max_results)()
+        n = check(self.lib.gd_server_poll(self.h, buf, max_results, timeout_ms))
+        out = []
+        for r in buf[:n]:
+            keep, rep, st = self._live.pop(r.ticket, (None, None, None))
+            out.append({"ticket": r.ticket, "status": r.status, "nrep": r.nrep, "steps": r.steps,
+                        "t_submit": r.t_submit, "t_admit": r.t_admit, "t_done": r.t_done,
+                        "replicas": rep, "stats": st})
+        return out
+
+    def drain(self, timeout_ms: int = -1) -> None:
+        check(self.lib.gd_server_drain(self.h, timeout_ms))
+
+    def stats(self) -> dict:
+        from ._lib import ServerStats
+
+        s = ServerStats()
+        check(self.lib.gd_server_get_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_ if k != "pad_"}
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.gd_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -196,6 +196,70 @@ int gd_ensemble_destroy(gd_ensemble_t *e);
 /* The CUDA stream (cudaStream_t) the ensemble launches on, for event timing. */
 void *gd_ensemble_stream(const gd_ensemble_t *e);
 
+/* ------------------------------------------------------------------ serving
+ * No counterpart in the reference (it runs one Complex per Dock call).  A
+ * server keeps pockets resident on one GPU and runs docking requests of any
+ * ligand size against them: requests queue, are admitted while the HBM
+ * budget, the replica cap and the job slots allow, and then share rounds (one
+ * persistent Monte Carlo launch over every admitted job, one exchange launch)
+ * with whatever else is running; finished requests leave between rounds and
+ * free their memory for the queue.  A request's result does not depend on
+ * the other requests (own seed, own step counter). */
+typedef struct gd_server gd_server_t;
+
+typedef struct gd_server_config {
+  unsigned long long hbm_budget_bytes; /* device bytes of admitted jobs (default 100 GB) */
+  int max_active_replicas;  /* replicas in one round (0: two waves of resident replica-warps) */
+  int max_jobs;             /* admitted jobs at a time (result staging slots), default 256 */
+  int max_replicas_per_job; /* default 1024 */
+  int max_atoms;            /* largest ligand accepted (sizes the per-warp buffers), default 128 */
+  int steps_per_round;      /* MC steps between scheduling decisions, default 50 */
+  int kde_stage;            /* KDE points staged in shared memory (more: read from global), default 1024 */
+  int warps;                /* replicas per CTA, 0: occupancy model */
+  int device;
+} gd_server_config_t;
+
+typedef struct gd_request {
+  const gd_job_desc_t *job;   /* job->pocket indexes the server's pockets   */
+  int steps;                  /* MC steps after the initial evaluation      */
+  int steps_per_exchange;     /* 0: no replica exchange                     */
+  ReplicaMC *replicas_out;    /* [nrep] final replica states, or NULL       */
+  double *stats_out;          /* [nrep][8] as gd_ensemble_stats, or NULL    */
+} gd_request_t;
+
+typedef struct gd_result {
+  long long ticket;
+  int status;                 /* GD_OK, or why the request failed           */
+  int nrep, steps, pad_;
+  double t_submit, t_admit, t_done; /* seconds on the server's clock        */
+} gd_result_t;
+
+typedef struct gd_server_stats {
+  long long submitted, completed, failed, queued, outstanding;
+  long long rounds, launches;       /* rounds run, kernels launched         */
+  double pose_evals;                /* replica-steps run (initial included) */
+  double device_ms;                 /* device time of the rounds            */
+  double now;                       /* the server's clock, seconds          */
+  unsigned long long used_bytes, peak_bytes;
+  int warps_per_cta, grid, max_active_replicas, pad_;
+} gd_server_stats_t;
+
+void gd_server_config_default(gd_server_config_t *cfg);
+/* Pockets are packed once and stay resident until gd_server_destroy. */
+int gd_server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *enepara,
+                     const gd_server_config_t *cfg, gd_server_t **out);
+/* Validates and queues a request (the job is copied; its output buffers must
+ * stay valid until its result is polled).  Thread-safe. */
+int gd_server_submit(gd_server_t *s, const gd_request_t *req, long long *ticket);
+/* Up to max finished requests; waits up to timeout_ms (-1: until one is
+ * ready or nothing is outstanding).  Returns the count (>= 0). */
+int gd_server_poll(gd_server_t *s, gd_result_t *out, int max, int timeout_ms);
+/* Waits until every submitted request finished (-1: no limit). */
+int gd_server_drain(gd_server_t *s, int timeout_ms);
+int gd_server_get_stats(gd_server_t *s, gd_server_stats_t *out);
+/* Stops the loop; requests not finished yet are cancelled. */
+int gd_server_destroy(gd_server_t *s);
+
 /* Measured FP32 FMA throughput of the current GPU (TFLOP/s, 2 flops per FMA):
  * the denominator of the pair kernel's roofline. */
 int gd_fp32_peak(double *tflops);

@@ -1,0 +1,117 @@
+"""The request loop (gd_server_*): results equal the resident-ensemble path bit
+for bit, each request's result is the same alone and in a mix of others that
+arrive while it runs, admission respects the HBM budget, and bad requests
+are refused at submission."""
+
+import time
+
+import numpy as np
+import pytest
+
+from geauxdock_b200 import dock, synth
+from geauxdock_b200._lib import GD_E_CAPACITY, GD_E_INVALID, GdockError
+
+pytestmark = pytest.mark.gpu
+
+
+def _pockets():
+    rng = np.random.default_rng(21)
+    return [synth.make_pocket(rng, 350, 2), synth.make_pocket(rng, 700, 3)]
+
+
+def _jobs(pockets, n, seed=5, sizes=(9, 33, 80, 17, 64, 45)):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        pi = i % len(pockets)
+        L = sizes[i % len(sizes)]
+        out.append(synth.make_job(rng, pockets[pi], L, 2, 150, 5, synth.ladder(4, 0.3, 3.0), seed=100 + i,
+                                  pocket_index=pi))
+    return out
+
+
+def _ensemble_result(pockets, job, enepara, steps, spx):
+    with dock.Ensemble.from_jobs(pockets, [job], enepara) as e:
+        e.init()
+        e.run(steps, spx)
+        e.sync()
+        return e.replicas(0), e.stats(0)
+
+
+def _serve(pockets, enepara, reqs, stagger_s=0.0, **cfg):
+    with dock.Server(pockets, enepara, **cfg) as srv:
+        tickets = []
+        for job, steps, spx in reqs:
+            tickets.append(srv.submit(job, steps, spx))
+            if stagger_s:
+                time.sleep(stagger_s)
+        srv.drain(120_000)
+        res = {r["ticket"]: r for r in srv.poll(len(reqs), 0)}
+        st = srv.stats()
+    assert len(res) == len(reqs)
+    return [res[t] for t in tickets], st
+
+
+def test_server_matches_ensemble(lib, enepara):
+    pockets = _pockets()
+    jobs = _jobs(pockets, 4)
+    reqs = [(jobs[0], 120, 50), (jobs[1], 75, 30), (jobs[2], 50, 50), (jobs[3], 0, 0)]
+    got, st = _serve(pockets, enepara, reqs, stagger_s=0.01)
+    for (job, steps, spx), r in zip(reqs, got):
+        assert r["status"] == 0 and r["steps"] == steps
+        rep, stats = _ensemble_result(pockets, job, enepara, steps, spx)
+        assert r["replicas"].tobytes() == rep.tobytes()
+        assert np.array_equal(r["stats"], stats)
+    assert st["completed"] == 4 and st["failed"] == 0 and st["outstanding"] == 0
+    nrep = [j.nlig * j.ntmp * pockets[j.pocket].nconf for j in jobs]
+    assert st["pose_evals"] == sum(n * (s + 1) for n, (_, s, _) in zip(nrep, reqs))
+
+
+def test_same_alone_and_in_mix(lib, enepara):
+    """A request gives the same bytes whether it runs alone or among requests
+    that arrive before and while it runs (different sizes, pockets, step counts)."""
+    pockets = _pockets()
+    jobs = _jobs(pockets, 7, seed=8)
+    probe = (jobs[3], 100, 25)
+    alone, _ = _serve(pockets, enepara, [probe])
+    mix_reqs = [(jobs[0], 150, 50), (jobs[1], 60, 20), probe, (jobs[2], 200, 50), (jobs[4], 30, 0),
+                (jobs[5], 80, 40), (jobs[6], 100, 25)]
+    mixed, st = _serve(pockets, enepara, mix_reqs, stagger_s=0.005, max_active_replicas=64)
+    assert alone[0]["replicas"].tobytes() == mixed[2]["replicas"].tobytes()
+    assert np.array_equal(alone[0]["stats"], mixed[2]["stats"])
+    assert all(r["status"] == 0 for r in mixed)
+    assert st["rounds"] >= 4
+
+
+def test_admission_respects_budget(lib, enepara):
+    """With room for one job at a time, each request is admitted only after the
+    previous one finished, in submission order."""
+    pockets = _pockets()
+    jobs = [j for j in _jobs(pockets, 6, seed=11) if j.pocket == 1][:3]
+    one = 400_000   # bytes: one of these jobs (about 280 kB each, mostly the psp gather) but not two
+    got, st = _serve(pockets, enepara, [(j, 60, 30) for j in jobs], hbm_budget_bytes=one)
+    for a, b in zip(got, got[1:]):
+        assert b["t_admit"] >= a["t_done"] - 1e-3
+    assert st["peak_bytes"] <= one
+
+
+def test_bad_requests_refused(lib, enepara):
+    pockets = _pockets()
+    job = _jobs(pockets, 1)[0]
+    with dock.Server(pockets, enepara, max_atoms=40, max_replicas_per_job=32) as srv:
+        big = _jobs(pockets, 3)[2]          # 80 atoms
+        with pytest.raises(GdockError) as ei:
+            srv.submit(big, 10)
+        assert ei.value.code == GD_E_CAPACITY
+        job.pocket = 5
+        with pytest.raises(GdockError) as ei:
+            srv.submit(job, 10)
+        assert ei.value.code == GD_E_INVALID
+        job.pocket = 0
+        with pytest.raises(GdockError) as ei:
+            srv.submit(job, -1)
+        assert ei.value.code == GD_E_INVALID
+        t = srv.submit(job, 10, 5)
+        srv.drain(60_000)
+        (r,) = srv.poll(4, 0)
+        assert r["ticket"] == t and r["status"] == 0

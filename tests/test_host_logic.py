@@ -81,3 +81,32 @@ def test_eval_rejects_bad_conformation_before_device_work(lib, enepara):
     with pytest.raises(GdockError) as ei:
         dock.eval_poses(cx, np.array([[0, 3]]), np.zeros((1, 6)))
     assert ei.value.code == GD_E_INVALID
+
+
+def test_server_defaults_and_validation(lib, enepara):
+    """Server configuration defaults; a bad configuration or a missing GPU is an
+    error status before any device work."""
+    import ctypes as C
+
+    from geauxdock_b200._lib import GD_E_INVALID, GD_E_NODEVICE, PocketDesc, ServerConfig
+
+    cfg = ServerConfig()
+    lib.gd_server_config_default(C.byref(cfg))
+    assert cfg.hbm_budget_bytes == 100 * 10**9 and cfg.steps_per_round == 50 and cfg.max_jobs == 256
+    keep: list = []
+    pk = synth.make_pocket(np.random.default_rng(3), 300, 2)
+    parr = (PocketDesc * 1)(synth.pocket_desc(pk, keep))
+    ep = np.array([enepara], dtype=Lo.ENEPARA)
+    h = C.c_void_p()
+    bad = ServerConfig()
+    lib.gd_server_config_default(C.byref(bad))
+    bad.steps_per_round = 0
+    assert lib.gd_server_create(parr, 1, C.c_void_p(ep.ctypes.data), C.byref(bad), C.byref(h)) == GD_E_INVALID
+    rc = lib.gd_server_create(parr, 1, C.c_void_p(ep.ctypes.data), C.byref(cfg), C.byref(h))
+    import torch
+
+    if not torch.cuda.is_available():
+        assert rc == GD_E_NODEVICE
+    else:
+        assert rc == 0
+        lib.gd_server_destroy(h)

@@ -71,3 +71,17 @@ def test_reference_layout_matches(oracle_lib):
     assert r.gdref_sizeof(b"Complex") == Lo.COMPLEX.itemsize
     assert r.gdref_sizeof(b"Record") == Lo.RECORD.itemsize
     assert r.gdref_sizeof(b"EnePara0") == Lo.ENEPARA0.itemsize
+
+
+def test_ctypes_mirrors_of_api_structs(lib):
+    """The ctypes structures of the serving and descriptor API match the C layout."""
+    import ctypes as C
+
+    from geauxdock_b200._lib import JobDesc, PocketDesc, Request, Result, ServerConfig, ServerStats, layout
+
+    for name, cls in (("gd_job_desc_t", JobDesc), ("gd_pocket_desc_t", PocketDesc),
+                      ("gd_server_config_t", ServerConfig), ("gd_request_t", Request),
+                      ("gd_result_t", Result), ("gd_server_stats_t", ServerStats)):
+        assert layout(f"sizeof.{name}") == C.sizeof(cls), name
+    assert layout("gd_server_stats_t.warps_per_cta") == ServerStats.warps_per_cta.offset
+    assert layout("gd_result_t.t_done") == Result.t_done.offset
