@@ -307,7 +307,7 @@ def run_serving(args, local: int) -> dict:
             if d > 0:
                 time.sleep(d)
             srv.submit(j, steps, STEPS_PER_INTERVAL, results=False)
-        srv.drain(-1)
+        srv.drain(900_000)
         res = srv.poll(len(batch), 0)
         assert len(res) == len(batch) and all(r["status"] == 0 for r in res), res[:2]
         lat = [r["t_done"] - r["t_submit"] for r in res]
@@ -320,7 +320,7 @@ def run_serving(args, local: int) -> dict:
     with dock.Server(pockets, ep, device=local, max_atoms=80) as srv:
         srv.submit(jobs[-1], 100, STEPS_PER_INTERVAL, results=False)   # warm-up
         srv.submit(jobs[-2], 100, STEPS_PER_INTERVAL, results=False)
-        srv.drain(-1)
+        srv.drain(900_000)
         srv.poll(4, 0)
         s0 = srv.stats()
         named = stream(srv, jobs[:n], args.serve_rate, 11)
