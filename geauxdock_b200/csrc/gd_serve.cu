@@ -333,7 +333,10 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
 }
 
 // Takes queued requests while the budget, the replica cap and the slots
-// allow (FIFO; the first request is always admitted into an idle server).
+// allow, in submission order.  A request alone always fits both (checked at
+// submission).  Memory of a finished request counts against the budget until
+// its result has been copied out; its replicas leave the cap when its last
+// round is enqueued.
 int admit(gd_server *s)
 {
   std::vector<std::unique_ptr<ServeReq>> take;
@@ -341,10 +344,9 @@ int admit(gd_server *s)
     std::lock_guard<std::mutex> lk(s->mu);
     while (!s->pending.empty()) {
       ServeReq &r = *s->pending.front();
-      const bool idle = s->active_reps == 0;
       if (s->free_slots.empty()) break;
-      if (!idle && s->active_reps + r.nrep > s->cfg.max_active_replicas) break;
-      if (!idle && s->used_bytes + r.bytes > s->cfg.hbm_budget_bytes) break;
+      if (s->active_reps + r.nrep > s->cfg.max_active_replicas) break;
+      if (s->used_bytes + r.bytes > s->cfg.hbm_budget_bytes) break;
       s->used_bytes += r.bytes;
       s->stats.peak_bytes = std::max(s->stats.peak_bytes, (unsigned long long)s->used_bytes);
       s->active_reps += r.nrep;
