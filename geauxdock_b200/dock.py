@@ -208,7 +208,8 @@ class Server:
         return t.value
 
     def _nconf(self, pocket: int) -> int:
-        return self._pocket_nconf[pocket]
+        # an out-of-range index is refused by gd_server_submit
+        return self._pocket_nconf[pocket] if 0 <= pocket < len(self._pocket_nconf) else 0
 
     def poll(self, max_results: int = 64, timeout_ms: int = -1) -> list:
         """Finished requests: dicts with ticket, status, times and (if kept) replicas / stats."""
