@@ -98,10 +98,13 @@ struct EnergyScratch {
 };
 static_assert(sizeof(EnergyScratch) == 192, "EnergyScratch size is part of the smem layout");
 
-// Running sums of the pair terms of one point row.
-template <typename T>
+// Running sums of the pair terms of one point row.  The electrostatic term
+// q_a q_p g(d) is summed per point as q_p * sum_a q_a g(d), one sum per point
+// the lane holds, and multiplied by q_p at the end of the row.
+template <typename T, int KPL>
 struct PairAcc {
-  T vdw, ele, pmf, psp, hdb;
+  T vdw, pmf, psp, hdb;
+  T ele[KPL];
 };
 
 // Scalar force-field constants of the pair terms, read once per pose.
@@ -119,17 +122,18 @@ struct PairConst {
 // Pair terms of ligand atoms [a, aend) (one type group) against the lane's
 // KPL points, energy_prt_v1.cu:56-139 except the hydrophobic contact.  HDB /
 // PSP: evaluate the hydrogen-bond / pocket-specific terms (some lane has a
-// non-zero parameter).  FP32 uses rearranged forms of the same formulas:
-//   p1 = p1a r^9, p2 = p2a r^6 with r = 1/d (one rsqrt),
-//   p4 = p1 (lj0 + lj0 lj1 d^2) + 1,
-//   g  = el0 + d^2 (a1 el1^2 + b1 el1^3 d) for el1 d < 1, else r/el1,
+// non-zero parameter).  FP32 uses rearranged forms of the same formulas
+// (t4 = (1/p1a, p2a/p1a, pmf0, pmf1), tab4_entry):
+//   LJ = (1 - (p2a/p1a) d^3) / (lj0 + lj0 lj1 d^2 + d^9 / p1a)   (divided through by p1),
+//   g  = el0 + d^2 (a1 el1^2 + b1 el1^3 d) for el1 d < 1, else r/el1 with r = 1/d,
 //   hdb1 exp(-((d - hdb0) hdb1)^2 / 2) = (hdb1 c) 2^-(d hdb1 c - hdb0 hdb1 c)^2 / c
-// (t2 = (hdb1 c, -hdb0 hdb1 c); the FP64 kernel gets t2 = (hdb0, hdb1)).
+// (t2 = (hdb1 c, -hdb0 hdb1 c)).  FP64 evaluates the reference's forms with
+// rf = (p1a, p2a, hdb0, hdb1).
 template <int PREC, int KPL, bool HDB, bool PSP, typename T>
 __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, const T (&px)[KPL],
-                                           const T (&py)[KPL], const T (&pz)[KPL], const T (&pe)[KPL],
-                                           const float4 (&t4)[KPL], const float2 (&t2)[KPL], const T (&tps)[KPL],
-                                           const PairConst &c, PairAcc<T> &acc)
+                                           const T (&py)[KPL], const T (&pz)[KPL], const float4 (&t4)[KPL],
+                                           const float2 (&t2)[KPL], const float4 (&rf)[KPL], const T (&tps)[KPL],
+                                           const PairConst &c, PairAcc<T, KPL> &acc)
 {
   if constexpr (PREC == kFP64) {
     const double lj0 = c.lj0, lj1 = c.lj1, el0 = c.el0, el1 = c.el1, a1 = c.a1, b1 = c.b1;
@@ -141,19 +145,19 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
         const double d2 = dx * dx + dy * dy + dz * dz;
         const double d4 = d2 * d2;
         const double d = sqrt(d2);
-        const double p1 = (double)t4[j].x / (d4 * d4 * d);
-        const double p2 = (double)t4[j].y / (d4 * d2);
+        const double p1 = (double)rf[j].x / (d4 * d4 * d);
+        const double p2 = (double)rf[j].y / (d4 * d2);
         const double p4 = p1 * lj0 * (1.0 + lj1 * d2) + 1.0;
         acc.vdw += (p1 - p2) / p4;
         const double s1 = el1 * d;
         const double g = (s1 < 1.0) ? el0 + a1 * s1 * s1 + b1 * s1 * s1 * s1 : 1.0 / s1;
-        acc.ele += la.w * pe[j] * g;
+        acc.ele[j] += la.w * g;
         const double dmp = d - (double)t4[j].z;
         acc.pmf += (double)t4[j].w / (1.0 + exp((-0.5 * d + 6.0) * dmp));
         if constexpr (PSP) acc.psp += (dmp <= 0.0) ? tps[j] : 0.0;
         if constexpr (HDB) {
-          const double h3 = (d - (double)t2[j].x) * (double)t2[j].y;
-          acc.hdb += (double)t2[j].y * exp(-0.5 * h3 * h3);
+          const double h3 = (d - (double)rf[j].z) * (double)rf[j].w;
+          acc.hdb += (double)rf[j].w * exp(-0.5 * h3 * h3);
         }
       }
     }
@@ -167,15 +171,13 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
         const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         const float r = rsqrt_approx(d2);
         const float d = d2 * r;
-        const float r2 = r * r;
-        const float r3 = r2 * r;
-        const float r6 = r3 * r3;
-        const float p1 = t4[j].x * (r6 * r3);
-        const float p2 = t4[j].y * r6;
-        const float p4 = fmaf(p1, fmaf(c.lj01, d2, c.lj0), 1.0f);
-        acc.vdw = fmaf(p1 - p2, rcp_approx(p4), acc.vdw);
+        const float d3 = d2 * d;
+        const float d6 = d3 * d3;
+        const float den = fmaf(d6 * d3, t4[j].x, fmaf(c.lj01, d2, c.lj0));
+        const float num = fmaf(-t4[j].y, d3, 1.0f);
+        acc.vdw = fmaf(num, rcp_approx(den), acc.vdw);
         const float g = (d2 < c.ed2) ? fmaf(d2, fmaf(c.eb, d, c.ea), c.el0) : r * c.inv_el1;
-        acc.ele = fmaf(la.w * pe[j], g, acc.ele);
+        acc.ele[j] = fmaf(la.w, g, acc.ele[j]);
         const float dmp = d - t4[j].z;
         const float ex = ex2_approx(fmaf(-0.5f * kLog2e, d, 6.0f * kLog2e) * dmp);
         acc.pmf = fmaf(t4[j].w, rcp_approx(1.0f + ex), acc.pmf);
@@ -254,6 +256,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     T px[KPL], py[KPL], pz[KPL], pe[KPL];
     int pt[KPL];
     uint32_t pm[KPL];
+    uint32_t ptbits = 0u, pmbits = 0u;
 #pragma unroll
     for (int j = 0; j < KPL; ++j) {
       const int p = row + 32 * j + lane;
@@ -261,32 +264,39 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
       pt[j] = __float_as_int(aux[p].y);
       pm[j] = __ldg(pmc + p);
+      ptbits |= 1u << pt[j];
+      pmbits |= pm[j];
     }
-    PairAcc<T> acc{0, 0, 0, 0, 0};
+    // point types present in the row, and ligand types with a pocket-specific
+    // potential on some point of it: decide per type group, for the whole warp,
+    // whether the sparse terms are evaluated
+    ptbits = __reduce_or_sync(0xffffffffu, ptbits);
+    pmbits = __reduce_or_sync(0xffffffffu, pmbits);
+    PairAcc<T, KPL> acc;
+    acc.vdw = acc.pmf = acc.psp = acc.hdb = 0;
+#pragma unroll
+    for (int j = 0; j < KPL; ++j) acc.ele[j] = 0;
     int a = 0;
     while (a < L) {
       const int2 grp = lgrp[a];
       const int lt = grp.x, aend = grp.y;
-      const uint32_t hm = par->hdbmask[lt];
-      float4 t4[KPL];
+      const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
+      const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
+      float4 t4[KPL], rf[KPL];
       float2 t2[KPL];
       T tps[KPL];
-      bool any_hdb = false, any_psp = false;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         t4[j] = par->tab4[lt][pt[j]];
+        if constexpr (PREC == kFP64) rf[j] = __ldg(J.ref4 + lt * kTabCols + pt[j]);
+        else rf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
         t2[j] = make_float2(0.f, 0.f);
         tps[j] = 0;
-        any_hdb |= ((hm >> pt[j]) & 1u) != 0u;
-        any_psp |= ((pm[j] >> lt) & 1u) != 0u;
       }
-      any_hdb = __any_sync(0xffffffffu, any_hdb);
-      any_psp = __any_sync(0xffffffffu, any_psp);
-      if (any_hdb) {
+      if constexpr (PREC != kFP64) {
+        if (any_hdb) {
 #pragma unroll
-        for (int j = 0; j < KPL; ++j) {
-          if constexpr (PREC == kFP64) t2[j] = __ldg(J.hdbref + lt * kTabCols + pt[j]);
-          else t2[j] = par->tab2[lt][pt[j]];
+          for (int j = 0; j < KPL; ++j) t2[j] = par->tab2[lt][pt[j]];
         }
       }
       if (any_psp) {
@@ -295,23 +305,26 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
       }
       if (any_hdb) {
-        if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
-        else pair_atoms<PREC, KPL, true, false>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+        if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+        else pair_atoms<PREC, KPL, true, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
       } else {
-        if (any_psp) pair_atoms<PREC, KPL, false, true>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
-        else pair_atoms<PREC, KPL, false, false>(lig, a, aend, px, py, pz, pe, t4, t2, tps, kc, acc);
+        if (any_psp) pair_atoms<PREC, KPL, false, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+        else pair_atoms<PREC, KPL, false, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
       }
       a = aend;
     }
+    T row_ele = 0;
+#pragma unroll
+    for (int j = 0; j < KPL; ++j) row_ele += pe[j] * acc.ele[j];
     if constexpr (PREC == kFP32Kahan) {
       kahan_add(s_vdw, c_vdw, acc.vdw);
-      kahan_add(s_ele, c_ele, acc.ele);
+      kahan_add(s_ele, c_ele, row_ele);
       kahan_add(s_pmf, c_pmf, acc.pmf);
       kahan_add(s_psp, c_psp, acc.psp);
       kahan_add(s_hdb, c_hdb, acc.hdb);
     } else {
       s_vdw += acc.vdw;
-      s_ele += acc.ele;
+      s_ele += row_ele;
       s_pmf += acc.pmf;
       s_psp += acc.psp;
       s_hdb += acc.hdb;

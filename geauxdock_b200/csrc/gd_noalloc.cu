@@ -54,12 +54,12 @@ struct NoAllocScratch {
   float2 aux[GD_MAX_CONF_PRT * GD_MAXPRO];
   float psp[GD_MAX_CONF_PRT * kLigTypes * GD_MAXPRO];
   uint32_t pspmask[GD_MAX_CONF_PRT * GD_MAXPRO];
-  float2 hdbref[kLigTypes * kTabCols];
+  float4 ref4[kLigTypes * kTabCols];
 };
 
 // field ids reported in info[1]
 enum { kFieldNLig = 1, kFieldNPrt, kFieldNatom, kFieldNatomConf, kFieldNpoint, kFieldKde, kFieldMcs, kFieldLigType,
-       kFieldPrtType, kFieldSeq3r, kFieldMcsRow };
+       kFieldPrtType, kFieldSeq3r, kFieldMcsRow, kFieldP1a };
 
 }  // namespace
 
@@ -142,16 +142,17 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
   for (int q = tid; q < kLigTypes * kTabCols; q += blockDim.x) {
     const int lt = q / kTabCols, pt = q % kTabCols;
     if (pt < kPadType) {
-      par.tab4[lt][pt] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
+      if (!(ep.p1a[lt][pt] > 0.f)) na_fail(S, kNaFailInput, kFieldP1a, q);
+      par.tab4[lt][pt] = tab4_entry(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
       const float h0 = ep.hdb0[lt][pt], h1 = ep.hdb1[lt][pt];
       const bool on = h0 > 0.1f;
       par.tab2[lt][pt] = on ? make_float2((float)((double)h1 * kHdbC), (float)(-(double)h0 * (double)h1 * kHdbC))
                             : make_float2(0.f, 0.f);
-      S->hdbref[q] = on ? make_float2(h0, h1) : make_float2(0.f, 0.f);
+      S->ref4[q] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], on ? h0 : 0.f, on ? h1 : 0.f);
     } else {
-      par.tab4[lt][pt] = make_float4(0.f, 0.f, 0.f, 0.f);
+      par.tab4[lt][pt] = tab4_padding();
       par.tab2[lt][pt] = make_float2(0.f, 0.f);
-      S->hdbref[q] = make_float2(0.f, 0.f);
+      S->ref4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
   for (int q = tid; q < kLigTypes; q += blockDim.x) {
@@ -266,7 +267,7 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     J.ntmp = 0;
     J.minus_beta = nullptr;
     J.par = &S->par;
-    J.hdbref = S->hdbref;
+    J.ref4 = S->ref4;
     J.nrep = 0;
     J.rep = nullptr;
     J.run_acc = nullptr;
@@ -398,6 +399,7 @@ const char *field_name(int f)
     case kFieldPrtType: return "a protein point type (index given)";
     case kFieldSeq3r: return "a class-2 point's seq3r (index given)";
     case kFieldMcsRow: return "an MCS row without any coordinate (row given)";
+    case kFieldP1a: return "enepara.p1a <= 0 (index lt * 32 + pt given; the pair kernel needs p1a > 0)";
     default: return "unknown field";
   }
 }

@@ -285,13 +285,17 @@ int job_from_desc(const gd_job_desc_t &d, int nprt, JobData &jd)
   return GD_OK;
 }
 
-void build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
+int build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
 {
   std::memset(&p, 0, sizeof(p));
   const double c = kHdbC;
   for (int lt = 0; lt < kLigTypes; ++lt) {
+    for (int pt = kPadType; pt < kTabCols; ++pt) p.tab4[lt][pt] = tab4_padding();
     for (int pt = 0; pt < GD_MAXTP1 && pt < kPadType; ++pt) {
-      p.tab4[lt][pt] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
+      if (!(ep.p1a[lt][pt] > 0.f))
+        return fail(GD_E_INVALID, "enepara: p1a[%d][%d] = %g (the pair kernel needs p1a > 0)", lt, pt,
+                    (double)ep.p1a[lt][pt]);
+      p.tab4[lt][pt] = tab4_entry(ep.p1a[lt][pt], ep.p2a[lt][pt], ep.pmf0[lt][pt], ep.pmf1[lt][pt]);
       // energy_prt_v1.cu:133-138 evaluates the hydrogen-bond term only where hdb0 > 0.1
       const float h0 = ep.hdb0[lt][pt], h1 = ep.hdb1[lt][pt];
       if (h0 > 0.1f) {
@@ -325,6 +329,7 @@ void build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
   p.ele_d2max = (float)(1.0 / ((double)ep.el1 * ep.el1));
   p.hdb_cinv = (float)(1.0 / c);
   for (int i = 0; i < 6; ++i) p.move_scale[i] = move_scale[i];
+  return GD_OK;
 }
 
 int pack_pocket(const PocketData &pk, DevPocket &out)
@@ -466,12 +471,15 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
     }
 
   DevParams par;
-  build_params(ep, jd.move_scale, par);
+  GD_TRY(build_params(ep, jd.move_scale, par));
   std::vector<DevParams> parv(1, par);
-  std::vector<float2> hdbref((size_t)kLigTypes * kTabCols, make_float2(0.f, 0.f));
+  std::vector<float4> ref4((size_t)kLigTypes * kTabCols, make_float4(0.f, 0.f, 0.f, 0.f));
   for (int lt = 0; lt < kLigTypes; ++lt)
-    for (int pt = 0; pt < kPadType; ++pt)
-      if (ep.hdb0[lt][pt] > 0.1f) hdbref[(size_t)lt * kTabCols + pt] = make_float2(ep.hdb0[lt][pt], ep.hdb1[lt][pt]);
+    for (int pt = 0; pt < kPadType; ++pt) {
+      const bool hb = ep.hdb0[lt][pt] > 0.1f;
+      ref4[(size_t)lt * kTabCols + pt] = make_float4(ep.p1a[lt][pt], ep.p2a[lt][pt], hb ? ep.hdb0[lt][pt] : 0.f,
+                                                     hb ? ep.hdb1[lt][pt] : 0.f);
+    }
 
   const int nrep = (int)jd.reps.size();
   std::vector<int> run_acc(nrep);
@@ -484,7 +492,7 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
 
   Arena ar;
   const size_t o_par = ar.put(parv), o_lig = ar.put(lig), o_lg = ar.put(lgrp), o_lc = ar.put(jd.lcenter);
-  const size_t o_pm = ar.put(pspmask), o_hr = ar.put(hdbref);
+  const size_t o_pm = ar.put(pspmask), o_hr = ar.put(ref4);
   const size_t o_kde = ar.put(kde), o_mcs = ar.put(mcs), o_tcc = ar.put(jd.tcc), o_psp = ar.put(psp);
   const size_t o_mb = ar.put(jd.minus_beta), o_rep = ar.put(jd.reps), o_acc = ar.put(run_acc), o_st = ar.put(stats);
   size_t o_rec = 0;
@@ -533,7 +541,7 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   J.ntmp = jd.ntmp;
   J.minus_beta = (const float *)(b + o_mb);
   J.par = (const DevParams *)(b + o_par);
-  J.hdbref = (const float2 *)(b + o_hr);
+  J.ref4 = (const float4 *)(b + o_hr);
   J.nrep = nrep;
   J.rep = (ReplicaMC *)(b + o_rep);
   J.run_acc = (int *)(b + o_acc);

@@ -90,7 +90,7 @@ int job_from_desc(const gd_job_desc_t &d, int nprt, JobData &jd);
 // Replica layout of SetReplica (src/frontend/util.C:371-406).
 void default_replicas(int nlig, int nprt, int ntmp, std::vector<ReplicaMC> &out);
 
-void build_params(const EnePara &ep, const float move_scale[6], DevParams &p);
+int build_params(const EnePara &ep, const float move_scale[6], DevParams &p);
 
 int pack_pocket(const PocketData &pk, DevPocket &out);
 // rec: external device Record array (nullptr with want_records allocates one).

@@ -151,10 +151,11 @@ __global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_be
                                      2.5f / 81.0f / 81.0f / 81.0f * d4 * d2 -
                                      0.5f / 81.0f / 81.0f / 81.0f / 81.0f * d4 * d4);
             ehpc1 += (d2 <= 81.0f) ? w.x * hp : 0.0f;
-            const float4 t4 = par.tab4[lt][pt];
-            const float2 t2 = __ldg(J.hdbref + lt * kTabCols + pt);
-            const float p1 = __fdividef(t4.x, d4 * d4 * d);
-            const float p2 = __fdividef(t4.y, d4 * d2);
+            const float4 t4 = par.tab4[lt][pt];                       // pmf0, pmf1 in .z, .w
+            const float4 rf = __ldg(J.ref4 + lt * kTabCols + pt);   // p1a, p2a, hdb0, hdb1
+            const float2 t2 = make_float2(rf.z, rf.w);
+            const float p1 = __fdividef(rf.x, d4 * d4 * d);
+            const float p2 = __fdividef(rf.y, d4 * d2);
             const float p4 = p1 * par.lj0 * (1.0f + par.lj1 * d2) + 1.0f;
             evdw += __fdividef(p1 - p2, p4);
             const float s1 = par.el1 * d;

@@ -181,6 +181,11 @@ def test_invalid_inputs_rejected(lib, enepara):
     bad[0]["mcs"][0]["x"][:] = Lo.MCS_INVALID_COORD   # an MCS row with no coordinate
     with pytest.raises(GdockError):
         dock.Ensemble.from_complexes([bad], [1])
+    bad = cx.copy()
+    bad[0]["enepara"]["p1a"][3, 7] = 0.0             # the FP32 pair form divides by p1a
+    with pytest.raises(GdockError) as ei:
+        dock.Ensemble.from_complexes([bad], [1])
+    assert ei.value.code == GD_E_INVALID
 
 
 def test_graph_replay_matches_launches(lib, enepara, oracle_lib):
