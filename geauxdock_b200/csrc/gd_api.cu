@@ -675,6 +675,109 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
 }
 
 // ------------------------------------------------------------ poses --
+// Energies of n poses of job `job` of a resident ensemble (mode 1 of the
+// batched kernel): poses grouped by protein conformation, one warp per pose.
+int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, int precision, float *out,
+            double *out64, float *raw)
+{
+  const DevJob &J = e->jobs[job].dj;
+  for (int i = 0; i < n; ++i)
+    if (conf[2 * i] < 0 || conf[2 * i] >= J.nlig || conf[2 * i + 1] < 0 || conf[2 * i + 1] >= J.nprt)
+      return fail(GD_E_INVALID, "pose %d: conformation (%d, %d) out of range", i, conf[2 * i], conf[2 * i + 1]);
+  const Options o = opts();
+  TileConfig tc{8, o.kpl, o.ab};
+  if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
+  int kst = J.nkde;
+  size_t smem = kernel_smem_bytes(e->Pmax, kst, e->lig_slots, tc.warps_per_cta, precision);
+  if (smem > kSmemLimit) {
+    kst = 0;
+    smem = kernel_smem_bytes(e->Pmax, kst, e->lig_slots, tc.warps_per_cta, precision);
+  }
+  if (smem > kSmemLimit) return fail(GD_E_CAPACITY, "pocket too large for shared memory");
+  // poses grouped by protein conformation so that a CTA stages one conformation
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return conf[2 * a + 1] < conf[2 * b + 1]; });
+  std::vector<int> sconf(2 * (size_t)n);
+  std::vector<float> smm(6 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    sconf[2 * i] = conf[2 * ord[i]];
+    sconf[2 * i + 1] = conf[2 * ord[i] + 1];
+    for (int k = 0; k < 6; ++k) smm[6 * i + k] = mm[6 * (size_t)ord[i] + k];
+  }
+  std::vector<WorkItem> items;
+  for (int i = 0; i < n;) {
+    int k = 1;
+    while (i + k < n && k < tc.warps_per_cta && sconf[2 * (i + k) + 1] == sconf[2 * i + 1]) ++k;
+    items.push_back(WorkItem{job, sconf[2 * i + 1], i, k});
+    i += k;
+  }
+  int *d_conf = nullptr;
+  float *d_mm = nullptr, *d_out = nullptr, *d_raw = nullptr;
+  double *d_out64 = nullptr;
+  WorkItem *d_items = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(d_conf);
+    cudaFree(d_mm);
+    cudaFree(d_out);
+    cudaFree(d_raw);
+    cudaFree(d_out64);
+    cudaFree(d_items);
+  };
+#define EV_CUDA(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t ce_ = (call);                                                                 \
+    if (ce_ != cudaSuccess) {                                                                 \
+      cleanup();                                                                              \
+      return fail(GD_E_CUDA, "pose evaluation: %s: %s", #call, cudaGetErrorString(ce_));      \
+    }                                                                                         \
+  } while (0)
+  EV_CUDA(cudaMalloc(&d_conf, sizeof(int) * 2 * n));
+  EV_CUDA(cudaMalloc(&d_mm, sizeof(float) * 6 * n));
+  EV_CUDA(cudaMalloc(&d_out, sizeof(float) * 10 * n));
+  if (raw) EV_CUDA(cudaMalloc(&d_raw, sizeof(float) * 9 * n));
+  if (out64) EV_CUDA(cudaMalloc(&d_out64, sizeof(double) * 10 * n));
+  EV_CUDA(cudaMalloc(&d_items, sizeof(WorkItem) * items.size()));
+  EV_CUDA(cudaMemcpyAsync(d_conf, sconf.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemcpyAsync(d_mm, smm.data(), sizeof(float) * 6 * n, cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, e->st));
+  EV_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
+  KArgs a{};
+  a.jobs = e->d_jobs;
+  a.items = d_items;
+  a.n_items = (int)items.size();
+  a.queue = e->d_queue;
+  a.err = e->d_err;
+  a.P = e->Pmax;
+  a.Kst = kst;
+  a.lig_slots = e->lig_slots;
+  a.conf = d_conf;
+  a.mm = d_mm;
+  a.out = d_out;
+  a.out64 = d_out64;
+  a.raw = d_raw;
+  int nsm = 0;
+  EV_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+  const int occ = std::max(1, kernel_occupancy(1, precision, tc, smem));
+  const int grid = std::max(1, std::min((int)items.size(), occ * nsm));
+  EV_CUDA(launch_kernel(1, precision, tc, a, grid, e->st));
+  std::vector<float> hout(10 * (size_t)n), hraw(raw ? 9 * (size_t)n : 0);
+  std::vector<double> hout64(out64 ? 10 * (size_t)n : 0);
+  EV_CUDA(cudaMemcpyAsync(hout.data(), d_out, sizeof(float) * 10 * n, cudaMemcpyDeviceToHost, e->st));
+  if (raw) EV_CUDA(cudaMemcpyAsync(hraw.data(), d_raw, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, e->st));
+  if (out64) EV_CUDA(cudaMemcpyAsync(hout64.data(), d_out64, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, e->st));
+  EV_CUDA(cudaStreamSynchronize(e->st));
+#undef EV_CUDA
+  for (int i = 0; i < n; ++i) {
+    const size_t o2 = (size_t)ord[i];
+    std::memcpy(out + 10 * o2, &hout[10 * (size_t)i], sizeof(float) * 10);
+    if (raw) std::memcpy(raw + 9 * o2, &hraw[9 * (size_t)i], sizeof(float) * 9);
+    if (out64) std::memcpy(out64 + 10 * o2, &hout64[10 * (size_t)i], sizeof(double) * 10);
+  }
+  cleanup();
+  return check_err(e);
+}
+
 int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int precision, float *out,
                   double *out64, float *raw)
 {
@@ -696,116 +799,22 @@ int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int
   e->jobs.resize(1);
   int rc = pack_pocket(pk, e->pockets[0]);
   if (rc == GD_OK) rc = pack_job(jd, e->pockets[0], c->enepara, false, nullptr, e->jobs[0]);
-  if (rc != GD_OK) {
-    destroy(e);
-    return rc;
+  if (rc == GD_OK) {
+    const DevJob &J = e->jobs[0].dj;
+    e->precision = precision;
+    e->Pmax = J.npoint_pad;
+    e->Kmax = J.nkde;
+    e->lig_slots = (J.natom + 3) & ~3;
+    rc = upload_jobs(e);
   }
-  const Options o = opts();
-  e->precision = precision;
-  const DevJob &J = e->jobs[0].dj;
-  e->Pmax = J.npoint_pad;
-  e->Kmax = J.nkde;
-  e->lig_slots = (J.natom + 3) & ~3;
-  TileConfig tc{8, o.kpl, o.ab};
-  if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
-  e->Kst = e->Kmax;
-  if (smem_for(e, tc.warps_per_cta, e->Kst) > kSmemLimit) e->Kst = 0;
-  e->smem = smem_for(e, tc.warps_per_cta, e->Kst);
-  if (e->smem > kSmemLimit) {
-    destroy(e);
-    return fail(GD_E_CAPACITY, "pocket too large for shared memory");
-  }
-  // poses grouped by protein conformation so that a CTA stages one conformation
-  std::vector<int> ord(n);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return conf[2 * a + 1] < conf[2 * b + 1]; });
-  std::vector<int> sconf(2 * (size_t)n);
-  std::vector<float> smm(6 * (size_t)n);
-  for (int i = 0; i < n; ++i) {
-    sconf[2 * i] = conf[2 * ord[i]];
-    sconf[2 * i + 1] = conf[2 * ord[i] + 1];
-    for (int k = 0; k < 6; ++k) smm[6 * i + k] = mm[6 * ord[i] + k];
-  }
-  std::vector<WorkItem> items;
-  for (int i = 0; i < n;) {
-    int k = 1;
-    while (i + k < n && k < tc.warps_per_cta && sconf[2 * (i + k) + 1] == sconf[2 * i + 1]) ++k;
-    items.push_back(WorkItem{0, sconf[2 * i + 1], i, k});
-    i += k;
-  }
-  int *d_conf = nullptr;
-  float *d_mm = nullptr, *d_out = nullptr, *d_raw = nullptr;
-  double *d_out64 = nullptr;
-  WorkItem *d_items = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(d_conf);
-    cudaFree(d_mm);
-    cudaFree(d_out);
-    cudaFree(d_raw);
-    cudaFree(d_out64);
-    cudaFree(d_items);
-    destroy(e);
-  };
-#define EV_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t ce_ = (call);                                                                 \
-    if (ce_ != cudaSuccess) {                                                                 \
-      cleanup();                                                                              \
-      return fail(GD_E_CUDA, "gd_eval_poses: %s: %s", #call, cudaGetErrorString(ce_));        \
-    }                                                                                         \
-  } while (0)
-  EV_CUDA(upload_jobs(e) == GD_OK ? cudaSuccess : cudaErrorUnknown);
-  EV_CUDA(cudaMalloc(&e->d_queue, sizeof(int)));
-  EV_CUDA(cudaMalloc(&e->d_err, sizeof(int)));
-  EV_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
-  EV_CUDA(cudaMalloc(&d_conf, sizeof(int) * 2 * n));
-  EV_CUDA(cudaMalloc(&d_mm, sizeof(float) * 6 * n));
-  EV_CUDA(cudaMalloc(&d_out, sizeof(float) * 10 * n));
-  if (raw) EV_CUDA(cudaMalloc(&d_raw, sizeof(float) * 9 * n));
-  if (out64) EV_CUDA(cudaMalloc(&d_out64, sizeof(double) * 10 * n));
-  EV_CUDA(cudaMalloc(&d_items, sizeof(WorkItem) * items.size()));
-  EV_CUDA(cudaMemcpyAsync(d_conf, sconf.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice, e->st));
-  EV_CUDA(cudaMemcpyAsync(d_mm, smm.data(), sizeof(float) * 6 * n, cudaMemcpyHostToDevice, e->st));
-  EV_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, e->st));
-  EV_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
-  EV_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), e->st));
-  KArgs a{};
-  a.jobs = e->d_jobs;
-  a.items = d_items;
-  a.n_items = (int)items.size();
-  a.queue = e->d_queue;
-  a.err = e->d_err;
-  a.P = e->Pmax;
-  a.Kst = e->Kst;
-  a.lig_slots = e->lig_slots;
-  a.conf = d_conf;
-  a.mm = d_mm;
-  a.out = d_out;
-  a.out64 = d_out64;
-  a.raw = d_raw;
-  int nsm = 0;
-  EV_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int occ = std::max(1, kernel_occupancy(1, precision, tc, e->smem));
-  const int grid = std::max(1, std::min((int)items.size(), occ * nsm));
-  EV_CUDA(launch_kernel(1, precision, tc, a, grid, e->st));
-  std::vector<float> hout(10 * (size_t)n), hraw(raw ? 9 * (size_t)n : 0);
-  std::vector<double> hout64(out64 ? 10 * (size_t)n : 0);
-  EV_CUDA(cudaMemcpyAsync(hout.data(), d_out, sizeof(float) * 10 * n, cudaMemcpyDeviceToHost, e->st));
-  if (raw) EV_CUDA(cudaMemcpyAsync(hraw.data(), d_raw, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, e->st));
-  if (out64) EV_CUDA(cudaMemcpyAsync(hout64.data(), d_out64, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, e->st));
-  EV_CUDA(cudaStreamSynchronize(e->st));
-  int herr = 0;
-  EV_CUDA(cudaMemcpy(&herr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-#undef EV_CUDA
-  for (int i = 0; i < n; ++i) {
-    const int o = ord[i];
-    std::memcpy(out + 10 * (size_t)o, &hout[10 * (size_t)i], sizeof(float) * 10);
-    if (raw) std::memcpy(raw + 9 * (size_t)o, &hraw[9 * (size_t)i], sizeof(float) * 9);
-    if (out64) std::memcpy(out64 + 10 * (size_t)o, &hout64[10 * (size_t)i], sizeof(double) * 10);
-  }
-  cleanup();
-  if (herr) return fail(GD_E_TIMEOUT, "gd_eval_poses: bounded wait gave up");
-  return GD_OK;
+  if (rc == GD_OK && cudaMalloc(&e->d_queue, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMalloc");
+  if (rc == GD_OK && cudaMalloc(&e->d_err, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMalloc");
+  if (rc == GD_OK && cudaMemset(e->d_err, 0, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMemset");
+  if (rc == GD_OK && cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess)
+    rc = fail(GD_E_CUDA, "cudaStreamCreate");
+  if (rc == GD_OK) rc = eval_on(e, 0, n, conf, mm, precision, out, out64, raw);
+  destroy(e);
+  return rc;
 }
 
 // ---------------------------------------------------------- ensembles --
@@ -946,6 +955,18 @@ int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out)
   GD_CUDA(cudaMemcpyAsync(out, J.rep, sizeof(ReplicaMC) * (size_t)J.nrep, cudaMemcpyDeviceToHost, e->st));
   GD_CUDA(cudaStreamSynchronize(e->st));
   return GD_OK;
+}
+
+int gd_ensemble_eval_poses(gd_ensemble_t *e, int job, int n, const int *conf, const float *mm, int precision,
+                           float *out, double *out64, float *raw)
+{
+  if (!e || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  if (n < 0 || (n > 0 && (!conf || !mm || !out))) return fail(GD_E_INVALID, "null argument");
+  if (precision < GD_PREC_FP32 || precision > GD_PREC_FP64) return fail(GD_E_INVALID, "precision = %d", precision);
+  if (n == 0) return GD_OK;
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  return eval_on(e, job, n, conf, mm, precision, out, out64, raw);
 }
 
 int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8)

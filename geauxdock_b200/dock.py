@@ -141,6 +141,20 @@ class Ensemble:
         check(self.lib.gd_ensemble_stats(self.h, job, C.c_void_p(out.ctypes.data)))
         return out
 
+    def eval_poses(self, job: int, conf: np.ndarray, mm: np.ndarray, precision: int = GD_PREC_FP32,
+                   want64: bool = False, want_raw: bool = False):
+        """Energies of arbitrary poses of one job: (out [n,10] float32, raw [n,9] or None, out64 or None)."""
+        conf = np.ascontiguousarray(conf, dtype=np.int32).reshape(-1, 2)
+        mm = np.ascontiguousarray(mm, dtype=np.float32).reshape(-1, 6)
+        n = len(mm)
+        out = np.zeros((n, 10), np.float32)
+        raw = np.zeros((n, 9), np.float32) if want_raw else None
+        out64 = np.zeros((n, 10), np.float64) if want64 else None
+        check(self.lib.gd_ensemble_eval_poses(self.h, job, n, conf.ctypes.data, mm.ctypes.data, precision,
+                                              out.ctypes.data, None if out64 is None else out64.ctypes.data,
+                                              None if raw is None else raw.ctypes.data))
+        return out, raw, out64
+
     def autotune(self, steps: int = 4) -> str:
         buf = C.create_string_buffer(8192)
         check(self.lib.gd_ensemble_autotune(self.h, steps, buf, len(buf)))

@@ -190,6 +190,12 @@ int gd_ensemble_num_replicas(const gd_ensemble_t *e, int job);
 int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out);
 /* Per replica: {n_steps, n_accept, n_exch_try, n_exch_acc, mean E, var E, best E, best step}. */
 int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8);
+/* Energies of n arbitrary poses of job `job` (pose i: ligand conformation
+ * conf[2i], protein conformation conf[2i+1], movematrix mm[6i..6i+5]) with the
+ * resident pocket and job, in any precision; as gd_eval_poses for jobs beyond
+ * the Complex caps.  Waits for the ensemble's stream first. */
+int gd_ensemble_eval_poses(gd_ensemble_t *e, int job, int n, const int *conf, const float *mm, int precision,
+                           float *out, double *out64, float *raw);
 /* Choose the tile shape by timing candidates on a snapshot (state restored). */
 int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len);
 int gd_ensemble_destroy(gd_ensemble_t *e);

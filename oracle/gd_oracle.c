@@ -236,6 +236,143 @@ void gdo_energy(const Complex *c, int il, int ip, const float mm[6], double e[10
   e[9] = tot;
 }
 
+/* Cap-free twin of gdo_energy over descriptor arrays (the same formulas, the
+ * same file:line anchors); psp[lt][seq3r] from the job's [24][psp_ncol] table. */
+void gdo_energy_desc(const gd_pocket_desc_t *pk, const gd_job_desc_t *jb, const EnePara *ep, int il, int ip,
+                     const float mm[6], double e[10], double raw[9])
+{
+  const int L = jb->natom, P = pk->npoint, K = jb->nkde, M = jb->nmcs;
+  double rot[3][3];
+  rotation(mm, rot);
+  double *lx = (double *)malloc(sizeof(double) * 3 * (size_t)L);
+  const float *src = jb->lig_xyz + (size_t)il * L * 3;
+  const float *lcen = jb->lig_center + (size_t)il * 3;
+  const double tx = (double)mm[0] + (double)lcen[0];
+  const double ty = (double)mm[1] + (double)lcen[1];
+  const double tz = (double)mm[2] + (double)lcen[2];
+  for (int l = 0; l < L; ++l) {
+    const double a = src[3 * l], b = src[3 * l + 1], d = src[3 * l + 2];
+    lx[3 * l] = rot[0][0] * a + rot[0][1] * b + rot[0][2] * d + tx;
+    lx[3 * l + 1] = rot[1][0] * a + rot[1][1] * b + rot[1][2] * d + ty;
+    lx[3 * l + 2] = rot[2][0] * a + rot[2][1] * b + rot[2][2] * d + tz;
+  }
+  const float *pxyz = pk->xyz + (size_t)ip * P * 3;
+
+  /* protein-ligand pair terms, energy_prt_v1.cu:8-174 */
+  double evdw = 0, eele = 0, epmf = 0, epsp = 0, ehdb = 0, ehpc = 0;
+  const double lj0 = ep->lj0, lj1 = ep->lj1, el0 = ep->el0, el1 = ep->el1, a1 = ep->a1, b1 = ep->b1;
+  for (int l = 0; l < L; ++l) {
+    const int lt = jb->lig_type[l];
+    const double lc = jb->lig_charge[l];
+    double ehpc1 = 0.0;
+    for (int p = 0; p < P; ++p) {
+      const int pt = pk->type[p];
+      const double dx = lx[3 * l] - (double)pxyz[3 * p];
+      const double dy = lx[3 * l + 1] - (double)pxyz[3 * p + 1];
+      const double dz = lx[3 * l + 2] - (double)pxyz[3 * p + 2];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double d4 = d2 * d2;
+      const double d = sqrt(d2);
+      if (pk->cdc[p] == 1 && d2 <= 81.0) {
+        ehpc1 += (double)pk->hpp[p] *
+                 (1.0 - (3.5 / 81.0 * d2 - 4.5 / 81.0 / 81.0 * d4 + 2.5 / 81.0 / 81.0 / 81.0 * d4 * d2 -
+                         0.5 / 81.0 / 81.0 / 81.0 / 81.0 * d4 * d4));
+      }
+      const double p1 = (double)ep->p1a[lt][pt] / (d4 * d4 * d);
+      const double p2 = (double)ep->p2a[lt][pt] / (d4 * d2);
+      const double p4 = p1 * lj0 * (1.0 + lj1 * d2) + 1.0;
+      evdw += (p1 - p2) / p4;
+      const double s1 = el1 * d;
+      const double g1 = (s1 < 1.0) ? (el0 + a1 * s1 * s1 + b1 * s1 * s1 * s1) : (1.0 / s1);
+      eele += lc * (double)pk->ele[p] * g1;
+      const double dmp = d - (double)ep->pmf0[lt][pt];
+      epmf += (double)ep->pmf1[lt][pt] / (1.0 + exp((-0.5 * d + 6.0) * dmp));
+      if (pk->cls[p] == 2 && dmp <= 0.0) epsp += (double)jb->psp[(size_t)lt * jb->psp_ncol + pk->seq3r[p]];
+      const double hdb0 = ep->hdb0[lt][pt];
+      if (hdb0 > (double)0.1f) {
+        const double hdb1 = ep->hdb1[lt][pt];
+        const double h3 = (d - hdb0) * hdb1;
+        ehdb += hdb1 * exp(-0.5 * h3 * h3);
+      }
+    }
+    const double hpc2 = (ehpc1 - (double)ep->hpl0[lt]) / (double)ep->hpl1[lt];
+    ehpc += 0.5 * hpc2 * hpc2 - (double)ep->hpl2[lt];
+  }
+
+  /* KDE term, energy_kde_v1.cu:183-274 */
+  double ekde = 0.0;
+  for (int l = 0; l < L; ++l) {
+    const int lt = jb->lig_type[l];
+    double s = 0.0;
+    int n = 0;
+    for (int k = 0; k < K; ++k) {
+      if (jb->kde_type[k] != lt) continue;
+      const double dx = lx[3 * l] - (double)jb->kde_xyz[3 * k];
+      const double dy = lx[3 * l + 1] - (double)jb->kde_xyz[3 * k + 1];
+      const double dz = lx[3 * l + 2] - (double)jb->kde_xyz[3 * k + 2];
+      s += exp((double)ep->kde2 * (dx * dx + dy * dy + dz * dz));
+      ++n;
+    }
+    if (n != 0) ekde += s / (double)n;
+  }
+
+  /* MCS term, energy_mcs_v1.cu:277-320 */
+  double elhm = 0.0;
+  for (int m = 0; m < M; ++m) {
+    const float *row = jb->mcs_xyz + (size_t)m * L * 3;
+    double s = 0.0;
+    int n = 0;
+    for (int l = 0; l < L; ++l) {
+      if (row[3 * l] == GD_MCS_INVALID_COORD) continue;
+      const double dx = lx[3 * l] - (double)row[3 * l];
+      const double dy = lx[3 * l + 1] - (double)row[3 * l + 1];
+      const double dz = lx[3 * l + 2] - (double)row[3 * l + 2];
+      s += dx * dx + dy * dy + dz * dz;
+      ++n;
+    }
+    elhm += (double)jb->mcs_tcc[m] * sqrt(s / (double)n);
+  }
+
+  /* distance to the pocket centre, kernel_cuda_l1_montecarlo.cu:439-454 */
+  double dst = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    const double t = (double)lcen[i] + (double)mm[i] - (double)pk->center[3 * ip + i];
+    dst += t * t;
+  }
+  free(lx);
+
+  double r[9];
+  r[0] = evdw;
+  r[1] = eele;
+  r[2] = epmf;
+  r[3] = epsp;
+  r[4] = ehdb * (-1.0 / sqrt(2.0 * 3.14159265358979323846));
+  r[5] = ehpc;
+  r[6] = ekde / (double)ep->kde3;
+  r[7] = log(elhm / (double)M);
+  r[8] = sqrt(dst);
+  if (raw)
+    for (int i = 0; i < 9; ++i) raw[i] = r[i];
+  double tot = 0.0;
+  for (int i = 0; i < 9; ++i) {
+    double v = r[i];
+    if (i < 7) v /= (double)L;
+    v = (double)ep->a_para[i] * v + (double)ep->b_para[i];
+    e[i] = v;
+    tot += (double)ep->w[i] * v;
+  }
+  e[9] = tot;
+}
+
+void gdo_energy_desc_batch(const gd_pocket_desc_t *pk, const gd_job_desc_t *job, const EnePara *ep, int n,
+                           const int *conf, const float *mm, double *e, double *raw)
+{
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int i = 0; i < n; ++i)
+    gdo_energy_desc(pk, job, ep, conf[2 * i], conf[2 * i + 1], mm + 6 * (size_t)i, e + 10 * (size_t)i,
+                    raw ? raw + 9 * (size_t)i : NULL);
+}
+
 /* ----------------------------------------------------------- Monte Carlo -- */
 
 static int replica_step(Complex *c, Record *record, int r, int s, int s2max, uint64_t seed, int *run_acc)

@@ -16,6 +16,7 @@
 
 #include <stdint.h>
 #include "gdock_types.h"
+#include "gdock.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -33,6 +34,15 @@ float gdo_u01(uint32_t x);
  * ReplicaMC.energy; raw[0..8] (may be NULL) are the terms before the
  * per-atom division and the a/b normalisation. */
 void gdo_energy(const Complex *c, int il, int ip, const float mm[6], double e[10], double raw[9]);
+
+/* The same energy over cap-free dense arrays (gd_pocket_desc_t and
+ * gd_job_desc_t layouts): ligand conformation il, protein conformation ip.
+ * The ligand atoms are visited in input order for every term. */
+void gdo_energy_desc(const gd_pocket_desc_t *pk, const gd_job_desc_t *job, const EnePara *ep, int il, int ip,
+                     const float mm[6], double e[10], double raw[9]);
+/* n poses (conf[2i], conf[2i+1], mm[6i..]) with OpenMP over poses. */
+void gdo_energy_desc_batch(const gd_pocket_desc_t *pk, const gd_job_desc_t *job, const EnePara *ep, int n,
+                           const int *conf, const float *mm, double *e, double *raw);
 
 /* Monte Carlo over replicas [rep_begin, rep_end] for steps s1 .. s1+s2max-1,
  * with the draws of the GPU kernels (Philox keyed by seed).  s2max == 1 is the

@@ -44,6 +44,7 @@ def oracle() -> C.CDLL:
         lib.gdo_philox4x32_10.argtypes = [vp, vp, vp]
         lib.gdo_u01.argtypes = [C.c_uint32]
         lib.gdo_u01.restype = C.c_float
+        lib.gdo_energy_desc_batch.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp]
         _ora = lib
     return _ora
 
@@ -108,3 +109,21 @@ def ref_energies(cx: np.ndarray, reps: np.ndarray | None = None) -> np.ndarray:
     rec = Lo.aligned_zeros(Lo.RECORD, n)
     ref().gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, 1)
     return np.array(work[0]["replica"]["energy"][:n])
+
+
+def energy_desc(pocket, job, enepara: np.ndarray, conf: np.ndarray, mm: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """FP64 energies of n poses of a cap-free job (synth.Pocket / synth.Job): (e [n,10], raw [n,9])."""
+    from geauxdock_b200 import layout as Lo, synth
+
+    keep: list = []
+    pd = synth.pocket_desc(pocket, keep)
+    jd = synth.job_desc(job, keep)
+    ep = np.array([enepara], dtype=Lo.ENEPARA)
+    conf = np.ascontiguousarray(conf, dtype=np.int32)
+    mm = np.ascontiguousarray(mm, dtype=np.float32)
+    n = len(mm)
+    e = np.zeros((n, 10), np.float64)
+    raw = np.zeros((n, 9), np.float64)
+    oracle().gdo_energy_desc_batch(C.byref(pd), C.byref(jd), ep.ctypes.data, n, conf.ctypes.data, mm.ctypes.data,
+                                   e.ctypes.data, raw.ctypes.data)
+    return e, raw

@@ -1,0 +1,87 @@
+"""Precision study on the precision-study workload: random poses (uniform
+rotations, translations within 6 A of the cavity centre) of a 64-atom ligand
+against a 3000-point pocket with 1000 KDE points and 16 MCS templates.  Every
+term is evaluated on the GPU in FP32 with plain reductions, FP32 with
+compensated (Kahan) reductions and FP64; all poses are compared with the GPU
+FP64 kernel and a subsample with the FP64 CPU oracle.  Max and RMS relative
+error per term go to $GD_REPORT_DIR/precision_study.json when that is set.
+
+Relative error: |x - x64| / max(|x64|, 1) on the normalised terms e[0..9]
+(the scale the Metropolis test sees; terms near zero are compared in absolute
+terms), and |x - x64| / |x64| on the raw sums where |x64| > 1e-3."""
+
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+from geauxdock_b200 import dock, synth
+from geauxdock_b200._lib import GD_PREC_FP32, GD_PREC_FP32_KAHAN, GD_PREC_FP64
+
+pytestmark = pytest.mark.gpu
+
+N_POSES = 1_000_000      # FP32 and FP32 + Kahan
+N_FP64 = 131_072         # FP64 GPU kernel (the reference for the full set is this subset)
+N_ORACLE = 4096          # FP64 CPU oracle
+TERMS = ["vdw", "ele", "pmf", "psp", "hdb", "hpc", "kde", "lhm", "dst", "total"]
+TOL32 = 1e-5             # FP32 terms against FP64, in the normalised scale
+
+
+def _err(x, ref):
+    d = np.abs(np.asarray(x, np.float64) - ref)
+    return d / np.maximum(np.abs(ref), 1.0)
+
+
+def _raw_err(x, ref):
+    ok = np.abs(ref) > 1e-3
+    d = np.abs(np.asarray(x, np.float64) - ref) / np.where(ok, np.abs(ref), 1.0)
+    return np.where(ok, d, 0.0)
+
+
+def _stats(err):
+    return {t: {"max": float(err[:, i].max()), "rms": float(np.sqrt(np.mean(err[:, i] ** 2)))}
+            for i, t in enumerate(TERMS[:err.shape[1]])}
+
+
+def test_precision_study(lib, enepara, oracle_lib):
+    pk, job = synth.config4(1)
+    mm = synth.config4_poses(2, N_POSES)
+    conf = np.zeros((N_POSES, 2), np.int32)
+    res, secs = {}, {}
+    with dock.Ensemble.from_jobs([pk], [job], enepara) as e:
+        for name, prec, n in (("fp32", GD_PREC_FP32, N_POSES), ("fp32_kahan", GD_PREC_FP32_KAHAN, N_POSES),
+                              ("fp64", GD_PREC_FP64, N_FP64)):
+            e.eval_poses(0, conf[:64], mm[:64], prec)                 # warm-up
+            t0 = time.perf_counter()
+            out, raw, out64 = e.eval_poses(0, conf[:n], mm[:n], prec, want64=True, want_raw=True)
+            secs[name] = time.perf_counter() - t0
+            res[name] = (out64, raw)
+    sub = np.random.default_rng(3).choice(N_FP64, N_ORACLE, replace=False)
+    t0 = time.perf_counter()
+    e_or, raw_or = oracle_lib.energy_desc(pk, job, enepara, conf[sub], mm[sub])
+    secs["oracle_cpu"] = time.perf_counter() - t0
+
+    ref64 = res["fp64"][0]
+    report = {"workload": "64-atom ligand, 3000-point pocket, 1000 KDE points, 16 MCS templates; random poses",
+              "poses": {"fp32": N_POSES, "fp32_kahan": N_POSES, "fp64_gpu": N_FP64, "oracle_cpu": N_ORACLE},
+              "seconds": secs, "metric": "|x - x64| / max(|x64|, 1) on normalised terms"}
+    for name in ("fp32", "fp32_kahan", "fp64"):
+        e64, raw = res[name]
+        report[f"{name}_vs_oracle"] = _stats(_err(e64[sub], e_or))
+        report[f"{name}_vs_oracle_raw_rel"] = _stats(_raw_err(raw[sub], raw_or))
+        if name != "fp64":
+            report[f"{name}_vs_fp64_gpu"] = _stats(_err(e64[:N_FP64], ref64))
+    d = os.environ.get("GD_REPORT_DIR")
+    if d:
+        with open(os.path.join(d, "precision_study.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    print(json.dumps(report))
+
+    # FP64 on the GPU is the oracle's arithmetic up to summation order
+    assert max(v["max"] for v in report["fp64_vs_oracle"].values()) < 1e-9
+    for name in ("fp32", "fp32_kahan"):
+        worst = max(v["max"] for v in report[f"{name}_vs_oracle"].values())
+        assert worst <= TOL32, (name, report[f"{name}_vs_oracle"])
+        assert np.isfinite(res[name][0]).all()

@@ -155,3 +155,24 @@ def test_oracle_exchange_is_a_permutation(oracle_lib, enepara):
             a = sorted(map(tuple, before["energy"][idx].tolist()))
             b = sorted(map(tuple, after["energy"][idx].tolist()))
             assert a == b
+
+
+def test_cap_free_oracle_matches_complex_oracle(oracle_lib, enepara):
+    """The descriptor-based FP64 energy (used where a job exceeds the Complex
+    caps) equals the Complex-based one on a job that fits both, to FP64 rounding
+    (only the atom order of the KDE sum differs)."""
+    from geauxdock_b200 import synth
+
+    O = oracle_lib
+    rng = np.random.default_rng(12)
+    pk = synth.make_pocket(rng, 640, 2)
+    job = synth.make_job(rng, pk, 29, 3, 250, 7, synth.ladder(2, 0.3, 3.0), seed=3)
+    cx = synth.to_complex(job, pk, enepara)
+    n = 24
+    mm = synth.config4_poses(8, n, radius=4.0)
+    conf = np.stack([np.arange(n) % job.nlig, np.arange(n) % pk.nconf], axis=1).astype(np.int32)
+    e_desc, raw_desc = O.energy_desc(pk, job, enepara, conf, mm)
+    for i in range(n):
+        e, raw = O.energy(cx, int(conf[i, 0]), int(conf[i, 1]), mm[i])
+        assert np.allclose(e_desc[i], e, rtol=1e-12, atol=1e-12), (i, e_desc[i], e)
+        assert np.allclose(raw_desc[i], raw, rtol=1e-12, atol=1e-12)
