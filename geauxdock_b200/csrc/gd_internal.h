@@ -70,7 +70,8 @@ struct alignas(16) DevParams {
   float ele_a, ele_b, ele_d2max;      // a1 el1^2, b1 el1^3, 1/el1^2 (near-field branch: d^2 < 1/el1^2)
   float hdb_cinv;                     // 1/c
   float move_scale[6];
-  float pad_[2];
+  float kde3;                         // (h sqrt(2 pi))^3: the FP64 kernels divide by it
+  float pad_;
 };
 static_assert(sizeof(DevParams) % 16 == 0, "DevParams must be a multiple of 16 bytes");
 

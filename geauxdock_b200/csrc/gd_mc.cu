@@ -37,6 +37,7 @@ namespace {
 
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kSqrt2PiInvNeg = -0.3989422804014327f;  // -1/sqrt(2 pi), kernel_cuda_l1_montecarlo.cu:14
+constexpr double kSqrt2PiInvNegD = -0.39894228040143267794;  // the same in FP64
 constexpr uint32_t kWaitLimit = 1u << 26;
 
 // hydrophobic contact polynomial 1 - (3.5/81 d2 - 4.5/81^2 d4 + 2.5/81^3 d6 - 0.5/81^4 d8)
@@ -424,7 +425,9 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       }
     }
   }
-  const T ekde = warp_sum(kacc) * (T)par->kde3_inv;
+  T ekde;
+  if constexpr (PREC == kFP64) ekde = warp_sum(kacc) / (double)par->kde3;
+  else ekde = warp_sum(kacc) * par->kde3_inv;
 
   // ---- MCS, energy_mcs_v1.cu:277-320
   T macc = 0;
@@ -464,7 +467,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   r9[1] = ele;
   r9[2] = pmf;
   r9[3] = psp;
-  r9[4] = hdb * (T)kSqrt2PiInvNeg;
+  r9[4] = hdb * (PREC == kFP64 ? (T)kSqrt2PiInvNegD : (T)kSqrt2PiInvNeg);
   r9[5] = ehpc;
   r9[6] = ekde;
   r9[7] = log(elhm / (T)J.nmcs);

@@ -184,7 +184,8 @@ __global__ void na_setup_kernel(const Complex *__restrict__ cx, NoAllocScratch *
     par.ele_d2max = (float)(1.0 / ((double)ep.el1 * ep.el1));
     par.hdb_cinv = (float)(1.0 / kHdbC);
     for (int i = 0; i < 6; ++i) par.move_scale[i] = cx->mcpara.move_scale[i];
-    par.pad_[0] = par.pad_[1] = 0.f;
+    par.kde3 = ep.kde3;
+    par.pad_ = 0.f;
     // ligand atoms grouped by type, stable (the host packer's order)
     int k = 0;
     for (int t = 0; t < kLigTypes; ++t)

@@ -323,6 +323,7 @@ int build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
   p.b1 = ep.b1;
   p.kde2 = ep.kde2;
   p.kde3_inv = 1.0f / ep.kde3;  // kernel_cuda_l1_montecarlo.cu:194
+  p.kde3 = ep.kde3;
   p.lj01 = (float)((double)ep.lj0 * ep.lj1);
   p.ele_a = (float)((double)ep.a1 * ep.el1 * ep.el1);
   p.ele_b = (float)((double)ep.b1 * ep.el1 * ep.el1 * ep.el1);
