@@ -66,7 +66,7 @@ def _args():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--mc-steps", type=int, default=STEPS_PER_INTERVAL,
                    help="MC steps per bench step (= steps between exchange sweeps)")
-    p.add_argument("--tile", default="", help="warps,kpl,ab: fixed tile shape (skips the autotuner)")
+    p.add_argument("--tile", default="", help="warps,kpl,ab[,stage]: fixed tile shape (skips the autotuner)")
     p.add_argument("--skip-extras", action="store_true",
                    help="only the timed batched kernel (for profiling): no plain kernel, e2e, CPU baseline, "
                         "screening or serving legs")
@@ -377,7 +377,7 @@ def run_serving(args, local: int) -> dict:
                         "exchange every 50, 4 resident pockets (800/1500/2200/3000 points x 5), 100 GB HBM budget",
             "named_rate": named, "below_capacity": light, "plain_one_launch_per_request": plain,
             "speedup_over_plain": named["value"] / plain["value"],
-            "server": {"warps_per_cta": s2["warps_per_cta"], "grid": s2["grid"],
+            "server": {"warps_per_cta": s2["warps_per_cta"], "grid": s2["grid"], "pocket_staged": s2["pocket_staged"],
                        "max_active_replicas": s2["max_active_replicas"], "rounds": s2["rounds"],
                        "launches": s2["launches"], "peak_bytes": s2["peak_bytes"]},
             "sample": f"{named['requests']} + {light['requests']} requests (the named stream has 10000; "
@@ -418,10 +418,11 @@ def run_ours(args) -> None:
     # ---------------- resident ensemble, batched kernel
     check(lib.gd_set_option(b"kernel", 0))
     if args.tile:
-        w, kpl, ab = (int(x) for x in args.tile.split(","))
-        check(lib.gd_set_option(b"warps", w))
-        check(lib.gd_set_option(b"kpl", kpl))
-        check(lib.gd_set_option(b"ab", ab))
+        t = [int(x) for x in args.tile.split(",")]
+        check(lib.gd_set_option(b"warps", t[0]))
+        check(lib.gd_set_option(b"kpl", t[1]))
+        check(lib.gd_set_option(b"ab", t[2]))
+        check(lib.gd_set_option(b"stage", t[3] if len(t) > 3 else 1))
         args.no_autotune = True
     ens = dock.Ensemble.from_complexes([cx], [1000 + rank], device=local)
     ens.init()

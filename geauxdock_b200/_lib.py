@@ -78,7 +78,8 @@ class ServerStats(C.Structure):
         ("queued", C.c_longlong), ("outstanding", C.c_longlong), ("rounds", C.c_longlong),
         ("launches", C.c_longlong), ("pose_evals", C.c_double), ("device_ms", C.c_double), ("now", C.c_double),
         ("used_bytes", C.c_ulonglong), ("peak_bytes", C.c_ulonglong),
-        ("warps_per_cta", C.c_int), ("grid", C.c_int), ("max_active_replicas", C.c_int), ("pad_", C.c_int),
+        ("warps_per_cta", C.c_int), ("grid", C.c_int), ("max_active_replicas", C.c_int),
+        ("pocket_staged", C.c_int),
     ]
 
 

@@ -24,6 +24,7 @@ struct Options {
   int kpl = 2;
   int ab = 8;
   int graph = 1;  // replay whole exchange intervals from a captured graph
+  int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
 };
 Options g_opt;
 int g_ngpu = -1;
@@ -128,9 +129,9 @@ int build_items(gd_ensemble *e)
   return GD_OK;
 }
 
-size_t smem_for(const gd_ensemble *e, int warps, int kst)
+size_t smem_for(const gd_ensemble *e, int warps, int kst, int stage = 1)
 {
-  return kernel_smem_bytes(e->Pmax, kst, e->lig_slots, warps, e->precision);
+  return kernel_smem_bytes(stage ? e->Pmax : 0, kst, e->lig_slots, warps, e->precision);
 }
 
 // Pick the KDE staging, the grid and (if not given) the replicas per CTA.
@@ -138,11 +139,14 @@ int configure(gd_ensemble *e, TileConfig tc)
 {
   if (tc.warps_per_cta < 1 || tc.warps_per_cta * 32 > kMaxCtaThreads)
     return fail(GD_E_INVALID, "replicas per CTA = %d outside [1, %d]", tc.warps_per_cta, kMaxCtaThreads / 32);
+  // a pocket too large to stage is read through L1; KDE points that do not fit are read from global memory
+  if (tc.stage && smem_for(e, tc.warps_per_cta, 0, 1) > kSmemLimit) tc.stage = 0;
   e->Kst = e->Kmax;
-  if (smem_for(e, tc.warps_per_cta, e->Kst) > kSmemLimit) e->Kst = 0;  // KDE read from global memory
-  const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst);
+  if (smem_for(e, tc.warps_per_cta, e->Kst, tc.stage) > kSmemLimit) e->Kst = 0;
+  const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst, tc.stage);
   if (smem > kSmemLimit)
-    return fail(GD_E_CAPACITY, "pocket of %d points needs %zu B of shared memory (limit %zu)", e->Pmax, smem, kSmemLimit);
+    return fail(GD_E_CAPACITY, "%d replicas per CTA need %zu B of shared memory (limit %zu)", tc.warps_per_cta, smem,
+                kSmemLimit);
   const int occ = kernel_occupancy(0, e->precision, tc, smem);
   if (occ < 1) return fail(GD_E_INVALID, "tile (warps %d, kpl %d, ab %d) cannot launch", tc.warps_per_cta, tc.kpl, tc.ab);
   int nsm = 0;
@@ -160,18 +164,22 @@ int configure(gd_ensemble *e, TileConfig tc)
 
 // Replicas per CTA from occupancy: fewest waves of work items, then most
 // resident warps per SM.
-int choose_warps(gd_ensemble *e, TileConfig base)
+// stage_opt: -1 chooses between staging the pocket and reading it through L1.
+int choose_warps(gd_ensemble *e, TileConfig base, int stage_opt = -1)
 {
   int nsm = 0;
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
   double best = 1e300;
-  int best_w = 8;
+  int best_w = 8, best_stage = 1;
+  for (int stage = 1; stage >= 0; --stage)
   for (int w = 2; w <= kMaxCtaThreads / 32; ++w) {
+    if (stage_opt >= 0 && stage != stage_opt) continue;
     TileConfig tc = base;
     tc.warps_per_cta = w;
+    tc.stage = stage;
     int kst = e->Kmax;
-    if (smem_for(e, w, kst) > kSmemLimit) kst = 0;
-    const size_t smem = smem_for(e, w, kst);
+    if (smem_for(e, w, kst, stage) > kSmemLimit) kst = 0;
+    const size_t smem = smem_for(e, w, kst, stage);
     if (smem > kSmemLimit) continue;
     const int occ = kernel_occupancy(0, e->precision, tc, smem);
     if (occ < 1) continue;
@@ -191,14 +199,17 @@ int choose_warps(gd_ensemble *e, TileConfig base)
     const long long waves = (items + slots - 1) / slots;
     // time ~ waves * (warps resident per SM); fewer resident warps per SM than 16 also hurts latency hiding
     const int resident = occ * w;
-    const double t = (double)waves * std::max(resident, 16) / (double)std::min(resident, 32);
+    double t = (double)waves * std::max(resident, 16) / (double)std::min(resident, 32);
+    if (!stage) t *= 1.05;  // L1 reads of the pocket: prefer staging when occupancy is equal
     if (t < best - 1e-9) {
       best = t;
       best_w = w;
+      best_stage = stage;
     }
   }
   TileConfig tc = base;
   tc.warps_per_cta = best_w;
+  tc.stage = best_stage;
   return configure(e, tc);
 }
 
@@ -248,10 +259,10 @@ int finish_create(gd_ensemble *e)
   e->kernel = o.kernel;
   e->precision = o.precision;
   e->use_graph = o.graph != 0;
-  TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab};
+  TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab, o.stage != 0 ? 1 : 0};
   if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
   if (o.warps > 0) return configure(e, tc);
-  return choose_warps(e, tc);
+  return choose_warps(e, tc, o.stage);
 }
 
 int read_replica_prt(gd_ensemble *e, size_t j, const std::vector<ReplicaMC> &reps)
@@ -313,7 +324,7 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
   a.nsteps = nsteps;
   a.flags = flags;
   a.d_step = d_step;
-  a.P = e->Pmax;
+  a.P = e->tc.stage ? e->Pmax : 0;
   a.Kst = e->Kst;
   a.lig_slots = e->lig_slots;
   return a;
@@ -476,6 +487,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "ab") {
     if (v != 4 && v != 8) return fail(GD_E_INVALID, "ab = %lld", v);
     g_opt.ab = (int)v;
+  } else if (n == "stage") {
+    if (v < -1 || v > 1) return fail(GD_E_INVALID, "stage = %lld", v);
+    g_opt.stage = (int)v;
   } else if (n == "graph") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "graph = %lld", v);
     g_opt.graph = (int)v;
@@ -496,6 +510,7 @@ long long gd_get_option(const char *name)
   if (n == "kpl") return g_opt.kpl;
   if (n == "ab") return g_opt.ab;
   if (n == "graph") return g_opt.graph;
+  if (n == "stage") return g_opt.stage;
   return GD_E_INVALID;
 }
 
@@ -688,12 +703,14 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
   TileConfig tc{8, o.kpl, o.ab};
   if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
   int kst = J.nkde;
-  size_t smem = kernel_smem_bytes(e->Pmax, kst, e->lig_slots, tc.warps_per_cta, precision);
+  int P = e->Pmax;
+  if (kernel_smem_bytes(P, 0, e->lig_slots, tc.warps_per_cta, precision) > kSmemLimit) P = 0;  // through L1
+  size_t smem = kernel_smem_bytes(P, kst, e->lig_slots, tc.warps_per_cta, precision);
   if (smem > kSmemLimit) {
     kst = 0;
-    smem = kernel_smem_bytes(e->Pmax, kst, e->lig_slots, tc.warps_per_cta, precision);
+    smem = kernel_smem_bytes(P, kst, e->lig_slots, tc.warps_per_cta, precision);
   }
-  if (smem > kSmemLimit) return fail(GD_E_CAPACITY, "pocket too large for shared memory");
+  if (smem > kSmemLimit) return fail(GD_E_CAPACITY, "ligand slots too large for shared memory");
   // poses grouped by protein conformation so that a CTA stages one conformation
   std::vector<int> ord(n);
   std::iota(ord.begin(), ord.end(), 0);
@@ -748,7 +765,7 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
   a.n_items = (int)items.size();
   a.queue = e->d_queue;
   a.err = e->d_err;
-  a.P = e->Pmax;
+  a.P = P;
   a.Kst = kst;
   a.lig_slots = e->lig_slots;
   a.conf = d_conf;
@@ -1034,15 +1051,17 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   double best_t = 1e300;
   const int shapes[][2] = {{1, 8}, {2, 4}, {2, 8}, {4, 4}};
   const int warps[] = {4, 6, 8, 10, 12, 14, 16};
+  const bool can_stage = smem_for(e, 4, 0, 1) <= kSmemLimit;
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
+  for (int stage = can_stage ? 1 : 0; stage >= 0; --stage)
   for (const auto &sh : shapes) {
     if (e->precision == GD_PREC_FP64 && !(sh[0] == 1 && sh[1] == 8)) continue;
     for (int w : warps) {
       if (rc != GD_OK) break;
-      TileConfig tc{w, sh[0], sh[1]};
-      if (configure(e, tc) != GD_OK) continue;
+      TileConfig tc{w, sh[0], sh[1], stage};
+      if (configure(e, tc) != GD_OK || e->tc.stage != stage) continue;
       float t = 0;
       cudaEventRecord(a, e->st);
       rc = launch_mc(e, e->step, steps, 0);
@@ -1051,8 +1070,8 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
       cudaEventElapsedTime(&t, a, b);
       restore();
       char line[160];
-      snprintf(line, sizeof line, "warps=%d kpl=%d ab=%d grid=%d items=%d: %.3f ms\n", w, sh[0], sh[1], e->grid,
-               e->n_items, t);
+      snprintf(line, sizeof line, "warps=%d kpl=%d ab=%d stage=%d grid=%d items=%d: %.3f ms\n", w, sh[0], sh[1],
+               stage, e->grid, e->n_items, t);
       rep += line;
       if (t < best_t) {
         best_t = t;
@@ -1069,7 +1088,8 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   e->all_launches = 0;
   if (rc == GD_OK) rc = configure(e, best);
   char line[160];
-  snprintf(line, sizeof line, "chosen: warps=%d kpl=%d ab=%d\n", best.warps_per_cta, best.kpl, best.ab);
+  snprintf(line, sizeof line, "chosen: warps=%d kpl=%d ab=%d stage=%d\n", best.warps_per_cta, best.kpl, best.ab,
+           best.stage);
   rep += line;
   if (report && report_len > 0) {
     std::strncpy(report, rep.c_str(), (size_t)report_len - 1);

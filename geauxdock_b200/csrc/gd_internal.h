@@ -154,6 +154,7 @@ struct TileConfig {
   int warps_per_cta;   // replicas per CTA (one warp each)
   int kpl;             // pocket points per lane per row (1, 2 or 4)
   int ab;              // ligand atoms per register block (4 or 8)
+  int stage = 1;       // 1: stage the protein conformation in shared memory, 0: read it through L1
 };
 
 enum Precision { kFP32 = 0, kFP32Kahan = 1, kFP64 = 2 };
@@ -180,7 +181,7 @@ struct KArgs {
   int *err;
   int s_begin, nsteps, flags;
   const int *d_step;       // if set, steps start at *d_step + s_begin (graph replay)
-  int P, Kst, lig_slots;   // smem layout parameters (maximum over the launched jobs)
+  int P, Kst, lig_slots;   // smem layout (maxima over the launched jobs); P = 0: pocket read from global memory
   // pose evaluation
   const int *conf;
   const float *mm;

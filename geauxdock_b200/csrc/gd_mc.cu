@@ -501,14 +501,17 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
 {
   const int P = J.npoint_pad;
   const bool kde_in_smem = J.nkde <= A.Kst;
+  const bool pocket_in_smem = A.P > 0;
   if (threadIdx.x == 0) {
     fence_proxy_async_smem();
-    uint32_t bytes = (uint32_t)sizeof(DevParams) + 24u * (uint32_t)P;
+    uint32_t bytes = (uint32_t)sizeof(DevParams) + (pocket_in_smem ? 24u * (uint32_t)P : 0u);
     if (kde_in_smem) bytes += 16u * (uint32_t)J.nkde;
     mbar_expect_tx(bar, bytes);
     bulk_g2s(smem + sl.params, J.par, (uint32_t)sizeof(DevParams), bar);
-    bulk_g2s(smem + sl.pos, J.pos + (size_t)wi.prt * P, 16u * (uint32_t)P, bar);
-    bulk_g2s(smem + sl.aux, J.aux + (size_t)wi.prt * P, 8u * (uint32_t)P, bar);
+    if (pocket_in_smem) {
+      bulk_g2s(smem + sl.pos, J.pos + (size_t)wi.prt * P, 16u * (uint32_t)P, bar);
+      bulk_g2s(smem + sl.aux, J.aux + (size_t)wi.prt * P, 8u * (uint32_t)P, bar);
+    }
     if (kde_in_smem && J.nkde > 0) bulk_g2s(smem + sl.kde, J.kde, 16u * (uint32_t)J.nkde, bar);
   }
   int2 *lg = reinterpret_cast<int2 *>(smem + sl.lgrp);
@@ -560,8 +563,11 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     __syncthreads();
 
     const DevParams *par = reinterpret_cast<const DevParams *>(smem + sl.params);
-    const float4 *pos = reinterpret_cast<const float4 *>(smem + sl.pos);
-    const float2 *aux = reinterpret_cast<const float2 *>(smem + sl.aux);
+    // the protein conformation: staged in shared memory, or read through L1
+    const float4 *pos = A.P > 0 ? reinterpret_cast<const float4 *>(smem + sl.pos)
+                                : J.pos + (size_t)wi.prt * J.npoint_pad;
+    const float2 *aux = A.P > 0 ? reinterpret_cast<const float2 *>(smem + sl.aux)
+                                : J.aux + (size_t)wi.prt * J.npoint_pad;
     const float4 *kde = (J.nkde <= A.Kst) ? reinterpret_cast<const float4 *>(smem + sl.kde) : J.kde;
     const int2 *lgrp = reinterpret_cast<const int2 *>(smem + sl.lgrp);
     unsigned char *wbase = smem + sl.warp0 + (size_t)warp * sl.warp_bytes;

@@ -273,7 +273,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   a.jobs = s->d_jobs;
   a.queue = s->d_queue;
   a.err = s->d_err;
-  a.P = s->Pmax;
+  a.P = s->tc.stage ? s->Pmax : 0;
   a.Kst = s->Kst;
   a.lig_slots = s->lig_slots;
   int launches = 0;
@@ -435,32 +435,38 @@ int server_configure(gd_server *s)
   int nsm = 0;
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device));
   const int w0 = s->cfg.warps, wlo = w0 > 0 ? w0 : 2, whi = w0 > 0 ? w0 : kMaxCtaThreads / 32;
-  int best_w = 0, best_res = 0, best_occ = 0, best_kst = 0;
+  int best_w = 0, best_res = 0, best_occ = 0, best_kst = 0, best_stage = 1;
   size_t best_smem = 0;
+  // resident replica-warps per SM decide; the pocket is staged in shared
+  // memory unless reading it through L1 lets more replicas be resident
+  for (int stage = 1; stage >= 0; --stage)
   for (int w = wlo; w <= whi; ++w) {
     TileConfig tc = s->tc;
     tc.warps_per_cta = w;
+    tc.stage = stage;
+    const int P = stage ? s->Pmax : 0;
     int kst = s->cfg.kde_stage;
-    size_t smem = kernel_smem_bytes(s->Pmax, kst, s->lig_slots, w, s->precision);
+    size_t smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision);
     if (smem > kSmemLimitServe) {
       kst = 0;
-      smem = kernel_smem_bytes(s->Pmax, kst, s->lig_slots, w, s->precision);
+      smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision);
     }
     if (smem > kSmemLimitServe) continue;
     const int occ = kernel_occupancy(0, s->precision, tc, smem);
     if (occ < 1) continue;
     const int resident = std::min(occ * w, 32);
-    if (resident > best_res || (resident == best_res && kst > best_kst)) {
+    if (resident > best_res || (resident == best_res && stage == best_stage && kst > best_kst)) {
       best_res = resident;
       best_w = w;
       best_occ = occ;
       best_smem = smem;
       best_kst = kst;
+      best_stage = stage;
     }
   }
-  if (best_w == 0)
-    return fail(GD_E_CAPACITY, "pockets of up to %d points do not fit a launch (shared memory)", s->Pmax);
+  if (best_w == 0) return fail(GD_E_CAPACITY, "no launch shape fits shared memory");
   s->tc.warps_per_cta = best_w;
+  s->tc.stage = best_stage;
   s->Kst = best_kst;
   s->smem = best_smem;
   s->grid = best_occ * nsm;
@@ -667,6 +673,7 @@ int gd_server_get_stats(gd_server_t *s, gd_server_stats_t *out)
   out->outstanding = s->outstanding;
   out->used_bytes = s->used_bytes;
   out->warps_per_cta = s->tc.warps_per_cta;
+  out->pocket_staged = s->tc.stage;
   out->grid = s->grid;
   out->max_active_replicas = s->cfg.max_active_replicas;
   return GD_OK;

@@ -90,8 +90,10 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
 /* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*), "warps" (replicas
  * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape; default 2, 8),
  * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
- * 0: launch them one by one).  Applies to objects created afterwards on the
- * calling process. */
+ * 0: launch them one by one), "stage" (1: stage each protein conformation in
+ * shared memory, 0: read it through L1, -1: choose by occupancy; pockets too
+ * large to stage are always read through L1).  Applies to objects created
+ * afterwards on the calling process. */
 int gd_set_option(const char *name, long long value);
 long long gd_get_option(const char *name);
 
@@ -247,7 +249,8 @@ typedef struct gd_server_stats {
   double device_ms;                 /* device time of the rounds            */
   double now;                       /* the server's clock, seconds          */
   unsigned long long used_bytes, peak_bytes;
-  int warps_per_cta, grid, max_active_replicas, pad_;
+  int warps_per_cta, grid, max_active_replicas;
+  int pocket_staged;                /* 1: pockets staged in shared memory, 0: read through L1 */
 } gd_server_stats_t;
 
 void gd_server_config_default(gd_server_config_t *cfg);

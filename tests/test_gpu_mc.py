@@ -135,11 +135,14 @@ def test_plain_kernel_matches_batched(lib, enepara):
 
 
 def test_reproducible_and_tile_independent(lib, enepara):
-    """Same seed -> bit-identical states, whatever the number of replicas per CTA."""
+    """Same seed -> bit-identical states, whatever the number of replicas per CTA
+    and whether the protein conformation is staged in shared memory or read
+    through L1."""
     cx = _small_ensemble(enepara, seed=2)
     out = []
-    for warps in (0, 3, 7):
+    for warps, stage in ((0, -1), (3, 1), (7, 1), (5, 0), (0, 0)):
         check(lib.gd_set_option(b"warps", warps))
+        check(lib.gd_set_option(b"stage", stage))
         try:
             with dock.Ensemble.from_complexes([cx], [21]) as ens:
                 ens.init()
@@ -148,6 +151,7 @@ def test_reproducible_and_tile_independent(lib, enepara):
                 out.append(ens.replicas(0))
         finally:
             check(lib.gd_set_option(b"warps", 0))
+            check(lib.gd_set_option(b"stage", -1))
     for o in out[1:]:
         assert o.tobytes() == out[0].tobytes()
 

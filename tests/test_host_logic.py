@@ -69,6 +69,9 @@ def test_options_validated(lib):
     assert lib.gd_get_option(b"kpl") == 4
     check(lib.gd_set_option(b"kpl", 2))
     assert lib.gd_get_option(b"graph") == 1
+    assert lib.gd_get_option(b"stage") == -1
+    with pytest.raises(GdockError):
+        check(lib.gd_set_option(b"stage", 2))
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"graph", 2))
 
