@@ -253,7 +253,7 @@ def run_screening(args, local: int) -> dict:
     pack_s = time.perf_counter() - t0
     ens.init()
     ens.sync()
-    tune = "" if args.no_autotune else ens.autotune(2)
+    tune = "" if args.no_autotune else ens.autotune(spi)
     ens.run(spi, spi)                    # warm-up: captures the interval graph
     ens.sync()
     stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
@@ -427,7 +427,7 @@ def run_ours(args) -> None:
     ens = dock.Ensemble.from_complexes([cx], [1000 + rank], device=local)
     ens.init()
     ens.sync()
-    tune = "" if args.no_autotune else ens.autotune(4)
+    tune = "" if args.no_autotune else ens.autotune(args.mc_steps)
     stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     spi = args.mc_steps

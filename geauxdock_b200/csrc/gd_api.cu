@@ -66,6 +66,7 @@ struct gd_ensemble {
   DevJob *d_jobs = nullptr;
   WorkItem *d_items = nullptr;
   int n_items = 0;
+  std::vector<WorkItem> h_items;   // host copy of d_items (the autotuner samples it)
   int *d_queue = nullptr;
   int *d_err = nullptr;
   int kernel = GD_KERNEL_BATCHED;
@@ -122,6 +123,7 @@ int build_items(gd_ensemble *e)
   if (e->d_items) cudaFree(e->d_items);
   e->d_items = nullptr;
   e->n_items = (int)sorted.size();
+  e->h_items = sorted;
   if (!sorted.empty()) {
     GD_CUDA(cudaMalloc(&e->d_items, sizeof(WorkItem) * sorted.size()));
     GD_CUDA(cudaMemcpy(e->d_items, sorted.data(), sizeof(WorkItem) * sorted.size(), cudaMemcpyHostToDevice));
@@ -1062,13 +1064,32 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
       if (rc != GD_OK) break;
       TileConfig tc{w, sh[0], sh[1], stage};
       if (configure(e, tc) != GD_OK || e->tc.stage != stage) continue;
+      // a strided sample of the work items (heaviest-first order kept), about two
+      // waves of the grid, so that a candidate runs the full chunk length
+      const int stride = std::max(1, e->n_items / std::max(1, 2 * e->grid));
+      std::vector<WorkItem> sample;
+      for (int i = 0; i < e->n_items; i += stride) sample.push_back(e->h_items[i]);
+      WorkItem *d_sample = nullptr;
+      if (cudaMalloc(&d_sample, sizeof(WorkItem) * sample.size()) != cudaSuccess ||
+          cudaMemcpyAsync(d_sample, sample.data(), sizeof(WorkItem) * sample.size(), cudaMemcpyHostToDevice,
+                          e->st) != cudaSuccess) {
+        cudaFree(d_sample);
+        rc = fail(GD_E_CUDA, "autotune sample");
+        break;
+      }
+      KArgs ka = mc_args(e, e->step, steps, 0, nullptr);
+      ka.items = d_sample;
+      ka.n_items = (int)sample.size();
       float t = 0;
+      cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st);
       cudaEventRecord(a, e->st);
-      rc = launch_mc(e, e->step, steps, 0);
+      const cudaError_t le = launch_kernel(0, e->precision, e->tc, ka, std::min(e->grid, ka.n_items), e->st);
       cudaEventRecord(b, e->st);
-      if (cudaStreamSynchronize(e->st) != cudaSuccess) rc = fail(GD_E_CUDA, "autotune launch");
+      if (le != cudaSuccess || cudaStreamSynchronize(e->st) != cudaSuccess) rc = fail(GD_E_CUDA, "autotune launch");
       cudaEventElapsedTime(&t, a, b);
+      cudaFree(d_sample);
       restore();
+      t *= (float)e->n_items / (float)sample.size();   // per whole launch
       char line[160];
       snprintf(line, sizeof line, "warps=%d kpl=%d ab=%d stage=%d grid=%d items=%d: %.3f ms\n", w, sh[0], sh[1],
                stage, e->grid, e->n_items, t);

@@ -198,7 +198,11 @@ int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8);
  * the Complex caps.  Waits for the ensemble's stream first. */
 int gd_ensemble_eval_poses(gd_ensemble_t *e, int job, int n, const int *conf, const float *mm, int precision,
                            float *out, double *out64, float *raw);
-/* Choose the tile shape by timing candidates on a snapshot (state restored). */
+/* Choose the tile shape (replicas per CTA, pair tile, pocket staging) by timing
+ * candidates on a snapshot of the state (restored after each).  steps: MC
+ * steps per launch to tune for (the chunk the caller runs, e.g. its exchange
+ * interval); each candidate runs them on a strided sample of about two waves
+ * of work items. */
 int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len);
 int gd_ensemble_destroy(gd_ensemble_t *e);
 /* The CUDA stream (cudaStream_t) the ensemble launches on, for event timing. */
