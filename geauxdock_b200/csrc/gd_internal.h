@@ -10,7 +10,7 @@
 //   pocket conformation  pos[P] float4 (x, y, z, ele), aux[P] float2 (hpp_eff,
 //                        type): hydrophobic-contact points first, each part
 //                        sorted by point type, padded with inert points
-//   force-field tables   tab4[24][32] float4 (1/p1a, p2a/p1a, pmf0, pmf1) for the FP32 pair loop
+//   force-field tables   tab4[24][32] float4 (1/p1a, -p2a/p1a, -pmf0, pmf1) for the FP32 pair loop
 //                        tab2[24][32] float2 (scaled hdb1, hdb0), unused pairs zeroed
 //                        ref4[24][32] float4 (p1a, p2a, hdb0, hdb1) as in EnePara (FP64, plain)
 //   ligand conformation  lig[L] float4 (x, y, z, charge), atoms grouped by type
@@ -45,20 +45,22 @@ constexpr double kHdbC = 0.8493218002880191;       // launch bound of the batche
 // Force-field parameters of one job, in the order the kernels stage them.
 // The FP32 pair code uses algebraically rearranged forms of the reference
 // formulas whose constants are precomputed here (values in the comments).
-// FP32 pair-table entry of one (ligand type, point type): the Lennard-Jones
-// term (p1 - p2) / (p1 lj0 (1 + lj1 d^2) + 1) with p1 = p1a / d^9, p2 = p2a / d^6
+// FP32 pair-table entry of one (ligand type, point type):
+// (1/p1a, -p2a/p1a, -pmf0, pmf1).  The Lennard-Jones term
+// (p1 - p2) / (p1 lj0 (1 + lj1 d^2) + 1) with p1 = p1a / d^9, p2 = p2a / d^6
 // divided through by p1 is (1 - (p2a/p1a) d^3) / (lj0 + lj0 lj1 d^2 + d^9 / p1a),
 // which needs p1a > 0 (true for every type pair of the reference's parameter
-// file; the packers refuse others).  Padding point types get 1/p1a = +inf:
-// the denominator is infinite and the term exactly zero.
+// file; the packers refuse others); d - pmf0 is d + (-pmf0), exactly.
+// Padding point types get 1/p1a = +inf: the denominator is infinite and every
+// term exactly zero.
 __host__ __device__ inline float4 tab4_entry(float p1a, float p2a, float pmf0, float pmf1)
 {
-  return make_float4((float)(1.0 / (double)p1a), (float)((double)p2a / (double)p1a), pmf0, pmf1);
+  return make_float4((float)(1.0 / (double)p1a), (float)(-(double)p2a / (double)p1a), -pmf0, pmf1);
 }
 __host__ __device__ inline float4 tab4_padding() { return make_float4(INFINITY, 0.f, 0.f, 0.f); }
 
 struct alignas(16) DevParams {
-  float4 tab4[kLigTypes][kTabCols];   // 1/p1a, p2a/p1a, pmf0, pmf1 (tab4_entry); the point-type
+  float4 tab4[kLigTypes][kTabCols];   // 1/p1a, -p2a/p1a, -pmf0, pmf1 (tab4_entry); the point-type
                                       // padding columns (>= 30) give exactly zero for every term
   float2 tab2[kLigTypes][kTabCols];   // hdb1*c, -hdb0*hdb1*c with c = sqrt(log2(e)/2);
                                       // zero where hdb0 <= 0.1 (no hydrogen-bond parameters)

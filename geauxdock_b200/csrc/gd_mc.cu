@@ -52,6 +52,16 @@ struct alignas(16) V4 {
   T x, y, z, w;
 };
 
+// FP32 ligand atom in shared memory with every value twice, so that packed
+// f32x2 arithmetic against two pocket points reads it as one register pair.
+struct alignas(16) LigAtom2 {
+  float2 x, y, z, q;
+};
+__device__ __forceinline__ V4<float> unpack(const LigAtom2 &a) { return V4<float>{a.x.x, a.y.x, a.z.x, a.q.x}; }
+__device__ __forceinline__ V4<double> unpack(const V4<double> &a) { return a; }
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 }  // namespace
@@ -77,7 +87,8 @@ __host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots,
   off = align16(off + 8u * (uint32_t)P);
   s.kde = off;
   off = align16(off + 16u * (uint32_t)Kst);
-  s.lig_bytes = (uint32_t)lig_slots * (fp64 ? 32u : 16u);
+  s.lig_bytes = (uint32_t)lig_slots * 32u;  // LigAtom2 (FP32) or V4<double> (FP64)
+  (void)fp64;
   // per warp: rotated ligand, ReplicaMC state, EnergyScratch (192 B), WarpStats (64 B)
   s.warp_bytes = align16(s.lig_bytes + (uint32_t)sizeof(ReplicaMC) + 192u + 64u);
   s.warp0 = off;
@@ -130,8 +141,8 @@ struct PairConst {
 //   hdb1 exp(-((d - hdb0) hdb1)^2 / 2) = (hdb1 c) 2^-(d hdb1 c - hdb0 hdb1 c)^2 / c
 // (t2 = (hdb1 c, -hdb0 hdb1 c)).  FP64 evaluates the reference's forms with
 // rf = (p1a, p2a, hdb0, hdb1).
-template <int PREC, int KPL, bool HDB, bool PSP, typename T>
-__device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, const T (&px)[KPL],
+template <int PREC, int KPL, bool HDB, bool PSP, typename T, typename LA>
+__device__ __forceinline__ void pair_atoms(const LA *lig, int a, int aend, const T (&px)[KPL],
                                            const T (&py)[KPL], const T (&pz)[KPL], const float4 (&t4)[KPL],
                                            const float2 (&t2)[KPL], const float4 (&rf)[KPL], const T (&tps)[KPL],
                                            const PairConst &c, PairAcc<T, KPL> &acc)
@@ -139,7 +150,7 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
   if constexpr (PREC == kFP64) {
     const double lj0 = c.lj0, lj1 = c.lj1, el0 = c.el0, el1 = c.el1, a1 = c.a1, b1 = c.b1;
     for (; a < aend; ++a) {
-      const V4<double> la = lig[a];
+      const V4<double> la = unpack(lig[a]);
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         const double dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -153,7 +164,7 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
         const double s1 = el1 * d;
         const double g = (s1 < 1.0) ? el0 + a1 * s1 * s1 + b1 * s1 * s1 * s1 : 1.0 / s1;
         acc.ele[j] += la.w * g;
-        const double dmp = d - (double)t4[j].z;
+        const double dmp = d + (double)t4[j].z;   // t4.z = -pmf0
         acc.pmf += (double)t4[j].w / (1.0 + exp((-0.5 * d + 6.0) * dmp));
         if constexpr (PSP) acc.psp += (dmp <= 0.0) ? tps[j] : 0.0;
         if constexpr (HDB) {
@@ -165,7 +176,7 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
   } else {
 #pragma unroll 2
     for (; a < aend; ++a) {
-      const V4<float> la = lig[a];
+      const V4<float> la = unpack(lig[a]);
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         const float dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -175,11 +186,11 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
         const float d3 = d2 * d;
         const float d6 = d3 * d3;
         const float den = fmaf(d6 * d3, t4[j].x, fmaf(c.lj01, d2, c.lj0));
-        const float num = fmaf(-t4[j].y, d3, 1.0f);
+        const float num = fmaf(t4[j].y, d3, 1.0f);
         acc.vdw = fmaf(num, rcp_approx(den), acc.vdw);
         const float g = (d2 < c.ed2) ? fmaf(d2, fmaf(c.eb, d, c.ea), c.el0) : r * c.inv_el1;
         acc.ele[j] = fmaf(la.w, g, acc.ele[j]);
-        const float dmp = d - t4[j].z;
+        const float dmp = d + t4[j].z;
         const float ex = ex2_approx(fmaf(-0.5f * kLog2e, d, 6.0f * kLog2e) * dmp);
         acc.pmf = fmaf(t4[j].w, rcp_approx(1.0f + ex), acc.pmf);
         if constexpr (PSP) acc.psp += (dmp <= 0.0f) ? tps[j] : 0.0f;
@@ -187,6 +198,68 @@ __device__ __forceinline__ void pair_atoms(const V4<T> *lig, int a, int aend, co
           const float h = fmaf(d, t2[j].x, t2[j].y);
           acc.hdb = fmaf(t2[j].x, ex2_approx(-(h * h)), acc.hdb);
         }
+      }
+    }
+  }
+}
+
+// Running sums of one point row in the packed form: component k of each
+// float2 belongs to point 2i + k of the lane's pair i.
+template <int KP>
+struct PairAcc2 {
+  float2 vdw[KP], pmf[KP], hdb[KP], ele[KP];
+  float psp;
+};
+
+// Per type group, per point pair: the table entries as register pairs.
+template <int KP>
+struct PairTab2 {
+  float2 inva[KP], nba[KP], npmf0[KP], pmf1[KP], h1c[KP], h0c[KP];
+};
+
+// Packed (f32x2) twin of the FP32 branch of pair_atoms: the same operations
+// in the same order, two pocket points per instruction (__ffma2_rn /
+// __fadd2_rn / __fmul2_rn, sm_100); the special functions stay per component.
+// npx/npy/npz hold the negated point coordinates (x_atom - x_point is
+// x_atom + (-x_point), exactly).
+template <int KP, bool HDB, bool PSP>
+__device__ __forceinline__ void pair_atoms_x2(const LigAtom2 *lig, int a, int aend, const float2 (&npx)[KP],
+                                              const float2 (&npy)[KP], const float2 (&npz)[KP],
+                                              const PairTab2<KP> &t, const float (&tps)[2 * KP],
+                                              const PairConst &c, PairAcc2<KP> &acc)
+{
+  const float2 lj01 = f2(c.lj01), lj0 = f2(c.lj0), one = f2(1.0f), inv_el1 = f2(c.inv_el1);
+  const float2 za = f2(-0.5f * kLog2e), zb = f2(6.0f * kLog2e);
+#pragma unroll 2
+  for (; a < aend; ++a) {
+    const LigAtom2 la = lig[a];
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+      const float2 dx = __fadd2_rn(la.x, npx[i]), dy = __fadd2_rn(la.y, npy[i]), dz = __fadd2_rn(la.z, npz[i]);
+      const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+      const float2 r = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
+      const float2 d = __fmul2_rn(d2, r);
+      const float2 d3 = __fmul2_rn(d2, d);
+      const float2 d6 = __fmul2_rn(d3, d3);
+      const float2 den = __ffma2_rn(__fmul2_rn(d6, d3), t.inva[i], __ffma2_rn(lj01, d2, lj0));
+      const float2 num = __ffma2_rn(t.nba[i], d3, one);
+      acc.vdw[i] = __ffma2_rn(num, make_float2(rcp_approx(den.x), rcp_approx(den.y)), acc.vdw[i]);
+      float2 g = __fmul2_rn(r, inv_el1);
+      if (d2.x < c.ed2) g.x = fmaf(d2.x, fmaf(c.eb, d.x, c.ea), c.el0);
+      if (d2.y < c.ed2) g.y = fmaf(d2.y, fmaf(c.eb, d.y, c.ea), c.el0);
+      acc.ele[i] = __ffma2_rn(la.q, g, acc.ele[i]);
+      const float2 dmp = __fadd2_rn(d, t.npmf0[i]);
+      const float2 z = __fmul2_rn(__ffma2_rn(za, d, zb), dmp);
+      const float2 e1 = __fadd2_rn(make_float2(ex2_approx(z.x), ex2_approx(z.y)), one);
+      acc.pmf[i] = __ffma2_rn(t.pmf1[i], make_float2(rcp_approx(e1.x), rcp_approx(e1.y)), acc.pmf[i]);
+      if constexpr (PSP) {
+        acc.psp += (dmp.x <= 0.0f) ? tps[2 * i] : 0.0f;
+        acc.psp += (dmp.y <= 0.0f) ? tps[2 * i + 1] : 0.0f;
+      }
+      if constexpr (HDB) {
+        const float2 h = __ffma2_rn(d, t.h1c[i], t.h0c[i]);
+        const float2 hh = __fmul2_rn(h, h);
+        acc.hdb[i] = __ffma2_rn(t.h1c[i], make_float2(ex2_approx(-hh.x), ex2_approx(-hh.y)), acc.hdb[i]);
       }
     }
   }
@@ -202,7 +275,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   const int lane = lane_id();
   const int L = J.natom;
   const int P = J.npoint_pad;
-  V4<T> *lig = reinterpret_cast<V4<T> *>(ligbuf);
+  using LA = typename std::conditional<PREC == kFP64, V4<double>, LigAtom2>::type;
+  LA *lig = reinterpret_cast<LA *>(ligbuf);
 
   // rotation + translation, kernel_cuda_l1_montecarlo.cu:336-380
   T r00, r01, r02, r10, r11, r12, r20, r21, r22;
@@ -237,7 +311,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     o.y = r10 * (T)v.x + r11 * (T)v.y + r12 * (T)v.z + ty;
     o.z = r20 * (T)v.x + r21 * (T)v.y + r22 * (T)v.z + tz;
     o.w = (T)v.w;
-    lig[a] = o;
+    if constexpr (PREC == kFP64) lig[a] = o;
+    else lig[a] = LigAtom2{f2(o.x), f2(o.y), f2(o.z), f2(o.w)};
   }
   __syncwarp();
 
@@ -253,82 +328,180 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   const uint32_t *pmc = J.pspmask + (size_t)iprt * P;
   const PairConst kc = PairConst::load(par);
 
-  for (int row = 0; row < P; row += 32 * KPL) {
-    T px[KPL], py[KPL], pz[KPL], pe[KPL];
-    int pt[KPL];
-    uint32_t pm[KPL];
-    uint32_t ptbits = 0u, pmbits = 0u;
-#pragma unroll
-    for (int j = 0; j < KPL; ++j) {
-      const int p = row + 32 * j + lane;
-      const float4 q = pos[p];
-      px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
-      pt[j] = __float_as_int(aux[p].y);
-      pm[j] = __ldg(pmc + p);
-      ptbits |= 1u << pt[j];
-      pmbits |= pm[j];
-    }
-    // point types present in the row, and ligand types with a pocket-specific
-    // potential on some point of it: decide per type group, for the whole warp,
-    // whether the sparse terms are evaluated
-    ptbits = __reduce_or_sync(0xffffffffu, ptbits);
-    pmbits = __reduce_or_sync(0xffffffffu, pmbits);
-    PairAcc<T, KPL> acc;
-    acc.vdw = acc.pmf = acc.psp = acc.hdb = 0;
-#pragma unroll
-    for (int j = 0; j < KPL; ++j) acc.ele[j] = 0;
-    int a = 0;
-    while (a < L) {
-      const int2 grp = lgrp[a];
-      const int lt = grp.x, aend = grp.y;
-      const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
-      const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
-      float4 t4[KPL], rf[KPL];
-      float2 t2[KPL];
-      T tps[KPL];
+  if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+    // packed form: the lane's points 2i and 2i+1 share one register pair
+    constexpr int KP = KPL / 2;
+    for (int row = 0; row < P; row += 32 * KPL) {
+      float2 npx[KP], npy[KP], npz[KP];
+      int pt[KPL];
+      uint32_t pm[KPL];
+      uint32_t ptbits = 0u, pmbits = 0u;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
-        t4[j] = par->tab4[lt][pt[j]];
-        if constexpr (PREC == kFP64) rf[j] = __ldg(J.ref4 + lt * kTabCols + pt[j]);
-        else rf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        t2[j] = make_float2(0.f, 0.f);
-        tps[j] = 0;
+        const int p = row + 32 * j + lane;
+        const float4 q = pos[p];
+        if (j & 1) {
+          npx[j / 2].y = -q.x; npy[j / 2].y = -q.y; npz[j / 2].y = -q.z;
+        } else {
+          npx[j / 2].x = -q.x; npy[j / 2].x = -q.y; npz[j / 2].x = -q.z;
+        }
+        pt[j] = __float_as_int(aux[p].y);
+        pm[j] = __ldg(pmc + p);
+        ptbits |= 1u << pt[j];
+        pmbits |= pm[j];
       }
-      if constexpr (PREC != kFP64) {
+      ptbits = __reduce_or_sync(0xffffffffu, ptbits);
+      pmbits = __reduce_or_sync(0xffffffffu, pmbits);
+      PairAcc2<KP> acc;
+#pragma unroll
+      for (int i = 0; i < KP; ++i) acc.vdw[i] = acc.pmf[i] = acc.hdb[i] = acc.ele[i] = f2(0.0f);
+      acc.psp = 0.0f;
+      int a = 0;
+      while (a < L) {
+        const int2 grp = lgrp[a];
+        const int lt = grp.x, aend = grp.y;
+        const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
+        const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
+        PairTab2<KP> tb;
+        float tps[KPL];
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+          const float4 t4 = par->tab4[lt][pt[j]];
+          if (j & 1) {
+            tb.inva[j / 2].y = t4.x; tb.nba[j / 2].y = t4.y; tb.npmf0[j / 2].y = t4.z; tb.pmf1[j / 2].y = t4.w;
+          } else {
+            tb.inva[j / 2].x = t4.x; tb.nba[j / 2].x = t4.y; tb.npmf0[j / 2].x = t4.z; tb.pmf1[j / 2].x = t4.w;
+          }
+          tps[j] = 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < KP; ++i) tb.h1c[i] = tb.h0c[i] = f2(0.0f);
         if (any_hdb) {
 #pragma unroll
-          for (int j = 0; j < KPL; ++j) t2[j] = par->tab2[lt][pt[j]];
+          for (int j = 0; j < KPL; ++j) {
+            const float2 t2 = par->tab2[lt][pt[j]];
+            if (j & 1) {
+              tb.h1c[j / 2].y = t2.x; tb.h0c[j / 2].y = t2.y;
+            } else {
+              tb.h1c[j / 2].x = t2.x; tb.h0c[j / 2].x = t2.y;
+            }
+          }
         }
-      }
-      if (any_psp) {
+        if (any_psp) {
 #pragma unroll
-        for (int j = 0; j < KPL; ++j)
-          if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+          for (int j = 0; j < KPL; ++j)
+            if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+        }
+        if (any_hdb) {
+          if (any_psp) pair_atoms_x2<KP, true, true>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+          else pair_atoms_x2<KP, true, false>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+        } else {
+          if (any_psp) pair_atoms_x2<KP, false, true>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+          else pair_atoms_x2<KP, false, false>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+        }
+        a = aend;
       }
-      if (any_hdb) {
-        if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
-        else pair_atoms<PREC, KPL, true, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+      float row_vdw = 0.f, row_ele = 0.f, row_pmf = 0.f, row_hdb = 0.f;
+#pragma unroll
+      for (int i = 0; i < KP; ++i) {
+        row_vdw += acc.vdw[i].x + acc.vdw[i].y;
+        row_pmf += acc.pmf[i].x + acc.pmf[i].y;
+        row_hdb += acc.hdb[i].x + acc.hdb[i].y;
+        // the point charges are read again here rather than held through the atom loop
+        row_ele += pos[row + 64 * i + lane].w * acc.ele[i].x + pos[row + 64 * i + 32 + lane].w * acc.ele[i].y;
+      }
+      if constexpr (PREC == kFP32Kahan) {
+        kahan_add(s_vdw, c_vdw, row_vdw);
+        kahan_add(s_ele, c_ele, row_ele);
+        kahan_add(s_pmf, c_pmf, row_pmf);
+        kahan_add(s_psp, c_psp, acc.psp);
+        kahan_add(s_hdb, c_hdb, row_hdb);
       } else {
-        if (any_psp) pair_atoms<PREC, KPL, false, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
-        else pair_atoms<PREC, KPL, false, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+        s_vdw += row_vdw;
+        s_ele += row_ele;
+        s_pmf += row_pmf;
+        s_psp += acc.psp;
+        s_hdb += row_hdb;
       }
-      a = aend;
     }
-    T row_ele = 0;
-#pragma unroll
-    for (int j = 0; j < KPL; ++j) row_ele += pe[j] * acc.ele[j];
-    if constexpr (PREC == kFP32Kahan) {
-      kahan_add(s_vdw, c_vdw, acc.vdw);
-      kahan_add(s_ele, c_ele, row_ele);
-      kahan_add(s_pmf, c_pmf, acc.pmf);
-      kahan_add(s_psp, c_psp, acc.psp);
-      kahan_add(s_hdb, c_hdb, acc.hdb);
-    } else {
-      s_vdw += acc.vdw;
-      s_ele += row_ele;
-      s_pmf += acc.pmf;
-      s_psp += acc.psp;
-      s_hdb += acc.hdb;
+  } else {
+    for (int row = 0; row < P; row += 32 * KPL) {
+      T px[KPL], py[KPL], pz[KPL], pe[KPL];
+      int pt[KPL];
+      uint32_t pm[KPL];
+      uint32_t ptbits = 0u, pmbits = 0u;
+  #pragma unroll
+      for (int j = 0; j < KPL; ++j) {
+        const int p = row + 32 * j + lane;
+        const float4 q = pos[p];
+        px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
+        pt[j] = __float_as_int(aux[p].y);
+        pm[j] = __ldg(pmc + p);
+        ptbits |= 1u << pt[j];
+        pmbits |= pm[j];
+      }
+      // point types present in the row, and ligand types with a pocket-specific
+      // potential on some point of it: decide per type group, for the whole warp,
+      // whether the sparse terms are evaluated
+      ptbits = __reduce_or_sync(0xffffffffu, ptbits);
+      pmbits = __reduce_or_sync(0xffffffffu, pmbits);
+      PairAcc<T, KPL> acc;
+      acc.vdw = acc.pmf = acc.psp = acc.hdb = 0;
+  #pragma unroll
+      for (int j = 0; j < KPL; ++j) acc.ele[j] = 0;
+      int a = 0;
+      while (a < L) {
+        const int2 grp = lgrp[a];
+        const int lt = grp.x, aend = grp.y;
+        const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
+        const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
+        float4 t4[KPL], rf[KPL];
+        float2 t2[KPL];
+        T tps[KPL];
+  #pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+          t4[j] = par->tab4[lt][pt[j]];
+          if constexpr (PREC == kFP64) rf[j] = __ldg(J.ref4 + lt * kTabCols + pt[j]);
+          else rf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+          t2[j] = make_float2(0.f, 0.f);
+          tps[j] = 0;
+        }
+        if constexpr (PREC != kFP64) {
+          if (any_hdb) {
+  #pragma unroll
+            for (int j = 0; j < KPL; ++j) t2[j] = par->tab2[lt][pt[j]];
+          }
+        }
+        if (any_psp) {
+  #pragma unroll
+          for (int j = 0; j < KPL; ++j)
+            if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+        }
+        if (any_hdb) {
+          if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+          else pair_atoms<PREC, KPL, true, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+        } else {
+          if (any_psp) pair_atoms<PREC, KPL, false, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+          else pair_atoms<PREC, KPL, false, false>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
+        }
+        a = aend;
+      }
+      T row_ele = 0;
+  #pragma unroll
+      for (int j = 0; j < KPL; ++j) row_ele += pe[j] * acc.ele[j];
+      if constexpr (PREC == kFP32Kahan) {
+        kahan_add(s_vdw, c_vdw, acc.vdw);
+        kahan_add(s_ele, c_ele, row_ele);
+        kahan_add(s_pmf, c_pmf, acc.pmf);
+        kahan_add(s_psp, c_psp, acc.psp);
+        kahan_add(s_hdb, c_hdb, acc.hdb);
+      } else {
+        s_vdw += acc.vdw;
+        s_ele += row_ele;
+        s_pmf += acc.pmf;
+        s_psp += acc.psp;
+        s_hdb += acc.hdb;
+      }
     }
   }
 
@@ -354,11 +527,36 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           px[j] = q.x; py[j] = q.y; pz[j] = q.z;
           ph[j] = aux[p].x;
         }
+        if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+          // packed form, the same operations per component
+          const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f), c2 = f2(-0.5f / 81.0f);
+#pragma unroll
+          for (int k = 0; k < AB; ++k) {
+            const int a = a0 + k;
+            if (a >= L) break;
+            const LigAtom2 la = lig[a];
+#pragma unroll
+            for (int i = 0; i < KPL / 2; ++i) {
+              const float2 dx = __fadd2_rn(la.x, make_float2(-px[2 * i], -px[2 * i + 1]));
+              const float2 dy = __fadd2_rn(la.y, make_float2(-py[2 * i], -py[2 * i + 1]));
+              const float2 dz = __fadd2_rn(la.z, make_float2(-pz[2 * i], -pz[2 * i + 1]));
+              const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+              float2 t = __ffma2_rn(d2, c1, one);
+              t.x = fmaxf(t.x, 0.0f);
+              t.y = fmaxf(t.y, 0.0f);
+              const float2 u = __ffma2_rn(d2, c2, one);
+              const float2 w = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, t), t), u);
+              hpc[k] = fmaf(ph[2 * i], w.x, hpc[k]);
+              hpc[k] = fmaf(ph[2 * i + 1], w.y, hpc[k]);
+            }
+          }
+          continue;
+        }
 #pragma unroll
         for (int k = 0; k < AB; ++k) {
           const int a = a0 + k;
           if (a >= L) break;
-          const V4<T> la = lig[a];
+          const V4<T> la = unpack(lig[a]);
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
             const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -414,7 +612,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       const int cnt = J.kcnt[lt];
       if (cnt == 0) continue;
       const int beg = J.kbeg[lt];
-      const V4<T> la = lig[a];
+      const V4<T> la = unpack(lig[a]);
       const T inv = (T)1 / (T)cnt;
       for (int k = beg + lane; k < beg + cnt; k += 32) {
         const float4 q = kde[k];
@@ -441,7 +639,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         for (int a = 0; a < L; ++a) {
           const float4 q = J.mcs[(size_t)a * M + m];
           if (q.w != 0.0f) {
-            const V4<T> la = lig[a];
+            const V4<T> la = unpack(lig[a]);
             const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
             s += dx * dx + dy * dy + dz * dz;
             ++n;
@@ -789,7 +987,7 @@ __global__ void __launch_bounds__(256) eval_global_kernel(const DevJob *jobp, co
   if (err != nullptr && *(volatile int *)err != 0) return;  // the job was not packed
   const DevJob &J = *jobp;
   const int warp = threadIdx.x >> 5, lane = lane_id();
-  const uint32_t lig_bytes = (uint32_t)kMaxAtoms * (PREC == kFP64 ? 32u : 16u);
+  const uint32_t lig_bytes = (uint32_t)kMaxAtoms * 32u;
   unsigned char *wb = smem + (size_t)warp * (lig_bytes + sizeof(EnergyScratch));
   EnergyScratch *esc = reinterpret_cast<EnergyScratch *>(wb + lig_bytes);
   const int nwarps = gridDim.x * (blockDim.x >> 5);
@@ -815,7 +1013,7 @@ cudaError_t launch_eval_global(int precision, const DevJob *d_job, const int *co
                                float *out, float *raw, int *err, int grid, cudaStream_t st)
 {
   const int threads = 256;
-  const size_t smem = (size_t)(threads / 32) * ((size_t)kMaxAtoms * (precision == kFP64 ? 32 : 16) + sizeof(EnergyScratch));
+  const size_t smem = (size_t)(threads / 32) * ((size_t)kMaxAtoms * 32 + sizeof(EnergyScratch));
   if (n <= 0) return cudaSuccess;
   if (precision == kFP32)
     eval_global_kernel<kFP32, 1, 8><<<grid, threads, smem, st>>>(d_job, conf, mm, n, out, raw, err);

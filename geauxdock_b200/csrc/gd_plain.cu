@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_be
             const float s1 = par.el1 * d;
             const float g1 = (s1 < 1.0f) ? (par.el0 + par.a1 * s1 * s1 + par.b1 * s1 * s1 * s1) : __fdividef(1.0f, s1);
             eele += la.w * q.w * g1;
-            const float dmp = d - t4.z;
+            const float dmp = d + t4.z;                               // t4.z = -pmf0
             epmf += __fdividef(t4.w, 1.0f + __expf((-0.5f * d + 6.0f) * dmp));
             if (dmp <= 0.0f) epsp += __ldg(pspc + (size_t)lt * P + p);
             if (t2.x > 0.1f) {
