@@ -25,6 +25,7 @@ struct Options {
   int ab = 8;
   int graph = 1;  // replay whole exchange intervals from a captured graph
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
+  int dock_cache = 1;  // Dock keeps its device state per GPU between calls
 };
 Options g_opt;
 int g_ngpu = -1;
@@ -51,10 +52,17 @@ constexpr int kExchTag = 1;
 
 }  // namespace
 
+struct gd_ensemble;
+
 struct gd_rng {
   uint64_t seed = 0;
   uint64_t calls = 0;
   int seeded = 0;
+  // Dock's resident state on this handle's GPU, kept between calls and refilled
+  // in place when the next Complex has the same shapes
+  gd_ensemble *dock = nullptr;
+  std::vector<unsigned char> dock_prt;  // protein bytes the cached pocket was packed from
+  Options dock_opt;                     // options the cached ensemble was configured with
 };
 
 struct gd_ensemble {
@@ -430,26 +438,112 @@ int ensemble_from_complex_range(const Complex *c, int rb, int re, uint64_t seed,
                                 gd_ensemble **out)
 {
   *out = nullptr;
+  Tracer tr("create");
   GD_TRY(set_device(device));
   PocketData pk;
   JobData jd;
   GD_TRY(pocket_from_complex(c, pk));
   GD_TRY(job_from_complex(c, rb, re, seed, jd));
+  tr.mark("read Complex");
   gd_ensemble *e = new gd_ensemble;
   e->device = device;
   e->pockets.resize(1);
   e->jobs.resize(1);
   int rc = pack_pocket(pk, e->pockets[0]);
+  tr.mark("pack pocket");
   if (rc == GD_OK) rc = pack_job(jd, e->pockets[0], c->enepara, rec != nullptr, rec, e->jobs[0]);
+  tr.mark("pack job");
   if (rc == GD_OK) {
     e->rep_prt.resize(1);
     read_replica_prt(e, 0, jd.reps);
     rc = finish_create(e);
   }
+  tr.mark("configure");
   if (rc != GD_OK) {
     destroy(e);
     return rc;
   }
+  *out = e;
+  return GD_OK;
+}
+
+// Dock's ensemble on GPU `device`: the handle's cached one refilled in place
+// when the shapes are unchanged (no allocation and no reconfiguration; the
+// packed pocket is kept when the protein bytes are unchanged), else a new one,
+// which the handle then keeps.
+int dock_ensemble(gd_rng *h, const Complex *c, int rb, int re, uint64_t seed, Record *rec, int device,
+                  gd_ensemble **out)
+{
+  *out = nullptr;
+  const Options o = opts();
+  const size_t prt_bytes = sizeof(Protein) * (size_t)std::max(0, std::min(c->size.n_prt, GD_MAX_CONF_PRT));
+  gd_ensemble *e = h->dock;
+  if (e && e->device == device && std::memcmp(&h->dock_opt, &o, sizeof(Options)) == 0 && e->jobs.size() == 1) {
+    Tracer tr("refill");
+    GD_TRY(set_device(device));
+    GD_CUDA(cudaStreamSynchronize(e->st));
+    JobData jd;
+    GD_TRY(job_from_complex(c, rb, re, seed, jd));
+    bool ok = true;
+    const bool same_prt =
+        h->dock_prt.size() == prt_bytes && std::memcmp(h->dock_prt.data(), c->prt, prt_bytes) == 0;
+    if (!same_prt) {
+      PocketData pk;
+      GD_TRY(pocket_from_complex(c, pk));
+      DevPocket np;
+      GD_TRY(pack_pocket(pk, np, &e->pockets[0], e->st));
+      if (np.arena != e->pockets[0].arena) {
+        free_pocket(np);
+        ok = false;
+      } else {
+        e->pockets[0] = np;
+        h->dock_prt.assign((const unsigned char *)c->prt, (const unsigned char *)c->prt + prt_bytes);
+      }
+    }
+    tr.mark("pocket");
+    if (ok) {
+      DevJobBuf nj;
+      GD_TRY(pack_job(jd, e->pockets[0], c->enepara, rec != nullptr, rec, nj, &e->jobs[0], e->st));
+      const DevJob &A = e->jobs[0].dj, &B = nj.dj;
+      if (nj.arena != e->jobs[0].arena) {
+        free_job(nj);
+        ok = false;
+      } else {
+        ok = A.natom == B.natom && A.nlig == B.nlig && A.nprt == B.nprt && A.ntmp == B.ntmp && A.nrep == B.nrep &&
+             A.nkde == B.nkde && A.nmcs == B.nmcs && A.npoint_pad == B.npoint_pad;
+        e->jobs[0] = nj;
+        std::vector<int> prt_of(jd.reps.size());
+        for (size_t r = 0; r < jd.reps.size(); ++r) prt_of[r] = jd.reps[r].idx_prt;
+        ok = ok && prt_of == e->rep_prt[0];
+      }
+    }
+    tr.mark("job");
+    if (ok) {
+      GD_CUDA(cudaMemcpyAsync(e->d_jobs, &e->jobs[0].dj, sizeof(DevJob), cudaMemcpyHostToDevice, e->st));
+      GD_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), e->st));
+      e->step = 0;
+      e->ev_used = 0;
+      e->launches = 0;
+      e->all_launches = 0;
+      *out = e;
+      return GD_OK;
+    }
+    destroy(e);  // shapes changed: a new ensemble below
+    h->dock = nullptr;
+    h->dock_prt.clear();
+  } else if (e) {
+    destroy(e);
+    h->dock = nullptr;
+    h->dock_prt.clear();
+  }
+  GD_TRY(ensemble_from_complex_range(c, rb, re, seed, rec, device, &e));
+  if (!o.dock_cache) {  // the caller destroys it after the call
+    *out = e;
+    return GD_OK;
+  }
+  h->dock = e;
+  h->dock_prt.assign((const unsigned char *)c->prt, (const unsigned char *)c->prt + prt_bytes);
+  h->dock_opt = o;
   *out = e;
   return GD_OK;
 }
@@ -492,6 +586,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "stage") {
     if (v < -1 || v > 1) return fail(GD_E_INVALID, "stage = %lld", v);
     g_opt.stage = (int)v;
+  } else if (n == "dock_cache") {
+    if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_cache = %lld", v);
+    g_opt.dock_cache = (int)v;
   } else if (n == "graph") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "graph = %lld", v);
     g_opt.graph = (int)v;
@@ -513,6 +610,7 @@ long long gd_get_option(const char *name)
   if (n == "ab") return g_opt.ab;
   if (n == "graph") return g_opt.graph;
   if (n == "stage") return g_opt.stage;
+  if (n == "dock_cache") return g_opt.dock_cache;
   return GD_E_INVALID;
 }
 
@@ -553,6 +651,7 @@ int DeviceFree(Complex **cd, Record **rd, gd_rng_t **rng)
   const int n = ngpu();
   for (int g = 0; g < n; ++g) {
     GD_CUDA(cudaSetDevice(g));
+    if (rng[g] && rng[g]->dock) destroy(rng[g]->dock);
     if (cd[g]) GD_CUDA(cudaFree(cd[g]));
     if (rd[g]) GD_CUDA(cudaFree(rd[g]));
     delete rng[g];
@@ -639,6 +738,7 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
   const int spx = (mp.steps_per_exchange > 0 && ch->size.n_tmp > 1) ? mp.steps_per_exchange : 0;
   std::vector<gd_ensemble *> ens(n, nullptr);
   int rc = GD_OK;
+  Tracer tr("Dock");
   for (int g = 0; g < n && rc == GD_OK; ++g) {
     if (!rng[g] || !cd[g] || !rd[g]) {
       rc = fail(GD_E_STATE, "Dock before DeviceAlloc/InitCurand on GPU %d", g);
@@ -646,13 +746,15 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
     }
     // each Dock call draws a fresh stream from the handle (the reference's curand state advances)
     const uint64_t seed = rng[g]->seed + (rng[g]->calls++ << 32);
-    rc = ensemble_from_complex_range(ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], g, &ens[g]);
+    rc = dock_ensemble(rng[g], ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], g, &ens[g]);
   }
+  tr.mark("pack+create");
   // initial energy, backend_gpu.cu:87-91: one step, no move, forced accept
   for (int g = 0; g < n && rc == GD_OK; ++g) {
     rc = set_device(g);
     if (rc == GD_OK) rc = launch_mc(ens[g], 0, 1, kMcInitial | kMcRecord | kMcResetRecord | kMcStoreAccept);
   }
+  tr.mark("initial (enqueued)");
   // dump chunks, backend_gpu.cu:96-114
   for (int s1 = 0; s1 < steps_total && rc == GD_OK; s1 += spd) {
     for (int g = 0; g < n && rc == GD_OK; ++g) {
@@ -673,6 +775,7 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
       }
       if (rc == GD_OK) rc = check_err(ens[g]);
     }
+    tr.mark("chunk + record copy");
   }
   // final replica states: device Complex (as the reference) and the host Complex
   for (int g = 0; g < n && rc == GD_OK; ++g) {
@@ -687,7 +790,16 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
         cudaStreamSynchronize(ens[g]->st) != cudaSuccess)
       rc = fail(GD_E_CUDA, "Dock final copy on GPU %d", g);
   }
-  for (int g = 0; g < n; ++g) destroy(ens[g]);
+  tr.mark("final replica copy");
+  for (int g = 0; g < n; ++g)
+    if (ens[g] && (!rng[g] || rng[g]->dock != ens[g])) destroy(ens[g]);  // not cached
+  if (rc != GD_OK)
+    for (int g = 0; g < n; ++g)
+      if (rng[g] && rng[g]->dock) {  // drop the cached state of a failed call
+        destroy(rng[g]->dock);
+        rng[g]->dock = nullptr;
+        rng[g]->dock_prt.clear();
+      }
   return rc;
 }
 

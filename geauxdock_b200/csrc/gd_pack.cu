@@ -10,6 +10,9 @@
 // with hdb0 <= 0.1 (energy_prt_v1.cu:134, hdb1 = 1/0 there) and the psp value
 // of points that are not class 2 (energy_prt_v1.cu:109).
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -52,6 +55,23 @@ inline float as_float(int i)
   return f;
 }
 }  // namespace
+
+namespace {
+double now_ms()
+{
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+Tracer::Tracer(const char *sc) : on(std::getenv("GDOCK_TRACE") != nullptr), scope(sc), t_last(now_ms()) {}
+
+void Tracer::mark(const char *phase)
+{
+  if (!on) return;
+  const double t = now_ms();
+  std::fprintf(stderr, "[gdock] %s %-24s %9.3f ms\n", scope, phase, t - t_last);
+  t_last = t;
+}
 
 int fail(int code, const char *fmt, ...)
 {
@@ -333,7 +353,7 @@ int build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
   return GD_OK;
 }
 
-int pack_pocket(const PocketData &pk, DevPocket &out)
+int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cudaStream_t st)
 {
   out = DevPocket{};
   const int n = pk.nconf;
@@ -381,8 +401,13 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
   }
   Arena ar;
   const size_t o_pos = ar.put(pos), o_aux = ar.put(aux), o_c = ar.put(pk.center), o_n = ar.put(ncdc);
-  GD_CUDA(cudaMalloc(&out.arena, ar.off));
-  GD_CUDA(cudaMemcpy(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice));
+  if (reuse && reuse->arena && reuse->bytes == ar.off) {
+    out.arena = reuse->arena;
+    GD_CUDA(cudaMemcpyAsync(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice, st));
+  } else {
+    GD_CUDA(cudaMalloc(&out.arena, ar.off));
+    GD_CUDA(cudaMemcpy(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice));
+  }
   out.bytes = ar.off;
   unsigned char *b = (unsigned char *)out.arena;
   out.pos = (float4 *)(b + o_pos);
@@ -394,7 +419,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out)
 
 namespace {
 int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
-                  cudaStream_t st, bool async, DevJobBuf &out)
+                  cudaStream_t st, bool async, DevJobBuf &out, const DevJobBuf *reuse = nullptr)
 {
   out = DevJobBuf{};
   const int L = jd.L;
@@ -500,7 +525,10 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   const bool alloc_rec = want_records && rec == nullptr;
   if (alloc_rec) o_rec = ar.take(sizeof(Record) * (size_t)nrep);
 
-  if (async) {
+  if (reuse && reuse->arena && reuse->bytes == ar.off && !alloc_rec) {
+    out.arena = reuse->arena;
+    GD_CUDA(cudaMemcpyAsync(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice, st));
+  } else if (async) {
     // stream-ordered: no device-wide synchronisation (a pageable copy may wait for `st` only)
     GD_CUDA(cudaMallocAsync(&out.arena, ar.off, st));
     if (alloc_rec) GD_CUDA(cudaMemsetAsync(out.arena, 0, ar.off, st));
@@ -558,9 +586,9 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
 }  // namespace
 
 int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
-             DevJobBuf &out)
+             DevJobBuf &out, const DevJobBuf *reuse, cudaStream_t st)
 {
-  return pack_job_impl(jd, pk, ep, want_records, rec, nullptr, false, out);
+  return pack_job_impl(jd, pk, ep, want_records, rec, st, false, out, reuse);
 }
 
 int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cudaStream_t st, DevJobBuf &out)

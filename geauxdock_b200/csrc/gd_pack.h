@@ -10,6 +10,16 @@
 
 namespace gd {
 
+// Phase timing on stderr when the environment variable GDOCK_TRACE is set:
+// host wall-clock milliseconds since the previous mark of the same tracer.
+struct Tracer {
+  explicit Tracer(const char *scope);
+  void mark(const char *phase);
+  bool on;
+  const char *scope;
+  double t_last;
+};
+
 // Sets the calling thread's error message; returns `code`.
 int fail(int code, const char *fmt, ...);
 
@@ -92,10 +102,13 @@ void default_replicas(int nlig, int nprt, int ntmp, std::vector<ReplicaMC> &out)
 
 int build_params(const EnePara &ep, const float move_scale[6], DevParams &p);
 
-int pack_pocket(const PocketData &pk, DevPocket &out);
+// reuse: a previous packing whose device arena is taken over (and refilled
+// with copies on `st`) when it has exactly the size the new packing needs;
+// otherwise a new arena is allocated and `reuse` is left to the caller.
+int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse = nullptr, cudaStream_t st = nullptr);
 // rec: external device Record array (nullptr with want_records allocates one).
 int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool want_records, Record *rec,
-             DevJobBuf &out);
+             DevJobBuf &out, const DevJobBuf *reuse = nullptr, cudaStream_t st = nullptr);
 // Stream-ordered variant (cudaMallocAsync + a copy on `st`), no records.
 int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cudaStream_t st, DevJobBuf &out);
 void free_pocket(DevPocket &p);

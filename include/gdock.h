@@ -92,8 +92,11 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
  * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
  * 0: launch them one by one), "stage" (1: stage each protein conformation in
  * shared memory, 0: read it through L1, -1: choose by occupancy; pockets too
- * large to stage are always read through L1).  Applies to objects created
- * afterwards on the calling process. */
+ * large to stage are always read through L1), "dock_cache" (1: Dock keeps
+ * its packed device state per GPU handle and refills it in place when the next
+ * Complex has the same shapes, keeping the packed protein when its bytes are
+ * unchanged; 0: everything is rebuilt and freed per call).  Applies to objects
+ * created afterwards on the calling process. */
 int gd_set_option(const char *name, long long value);
 long long gd_get_option(const char *name);
 

@@ -221,3 +221,34 @@ def test_graph_replay_matches_launches(lib, enepara, oracle_lib):
         got = np.frombuffer(out[1][j][0], dtype=Lo.REPLICA)
         same = _same_trajectory(got, ref[0]["replica"][:n])
         assert same.mean() >= 0.9, (j, same.mean())
+
+
+def test_dock_reuses_device_state(lib, enepara):
+    """Repeated Dock calls on one set of handles (same protein and new ligand;
+    new protein of the same shape; a new shape) give the same bytes whether
+    the device state is kept and refilled between calls or rebuilt each call."""
+    rng = np.random.default_rng(17)
+    pka = synth.make_pocket(rng, 300, 2)
+    pkb = synth.make_pocket(rng, 300, 2)
+    temps = np.array([0.4, 1.6], np.float32)
+    jobs = [synth.make_job(rng, pka, 20, 2, 100, 5, temps, seed=1),
+            synth.make_job(rng, pka, 20, 2, 100, 5, temps, seed=2),
+            synth.make_job(rng, pkb, 20, 2, 100, 5, temps, seed=3),
+            synth.make_job(rng, pkb, 27, 3, 90, 4, temps, seed=4)]
+    pks = [pka, pka, pkb, pkb]
+    cxs = [synth.to_complex(j, p, enepara, steps_total=100, steps_per_dump=50, steps_per_exchange=25)
+           for j, p in zip(jobs, pks)]
+    out = {}
+    try:
+        for cache in (1, 0):
+            check(lib.gd_set_option(b"dock_cache", cache))
+            res = []
+            with dock.DockSession(1, seed=5) as s:
+                for cx in cxs:
+                    w = cx.copy()
+                    rec = s.dock(w)
+                    res.append((w[0]["replica"].tobytes(), rec.tobytes()))
+            out[cache] = res
+    finally:
+        check(lib.gd_set_option(b"dock_cache", 1))
+    assert out[1] == out[0]

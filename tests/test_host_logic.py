@@ -70,6 +70,7 @@ def test_options_validated(lib):
     check(lib.gd_set_option(b"kpl", 2))
     assert lib.gd_get_option(b"graph") == 1
     assert lib.gd_get_option(b"stage") == -1
+    assert lib.gd_get_option(b"dock_cache") == 1
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"stage", 2))
     with pytest.raises(GdockError):
