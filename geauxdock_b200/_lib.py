@@ -39,6 +39,7 @@ EXPORTED = [
     "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy", "gd_ensemble_eval_poses",
+    "gd_replica_range", "gd_ensemble_create_complex_range",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
     "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
     "gd_server_config_default", "gd_server_create", "gd_server_submit", "gd_server_poll", "gd_server_drain",
@@ -142,6 +143,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_stats": (i, [vp, i, vp]), "gd_ensemble_autotune": (i, [vp, i, C.c_char_p, i]),
         "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),
         "gd_ensemble_eval_poses": (i, [vp, i, i, vp, vp, i, vp, vp, vp]),
+        "gd_replica_range": (i, [vp, i, i, ip, ip]),
+        "gd_ensemble_create_complex_range": (i, [vp, i, i, C.c_uint64, i, vp]),
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),
         "gd_eval_poses_noalloc": (i, [vp, i, vp, vp, i, vp, vp, vp]), "gd_noalloc_scratch_bytes": (C.c_size_t, []),

@@ -662,28 +662,64 @@ int DeviceFree(Complex **cd, Record **rd, gd_rng_t **rng)
   return GD_OK;
 }
 
-int SetParaT(Complex *ch, ParaT **pt)
+// Replicas per GPU of the split of prepair.C:366-392 (maximising balance);
+// with replica exchange on, cut at protein-conformation blocks so that exchange
+// partners (same protein and ligand conformation) stay on one GPU.
+static int split_per_gpu(const Complex *ch, int n, int *per_out)
 {
-  if (!ch || !pt) return fail(GD_E_INVALID, "null argument");
-  const int n = ngpu();
   const int n_rep = ch->size.n_rep;
+  if (n < 1) return fail(GD_E_INVALID, "ngpu = %d", n);
   if (n_rep < 1 || n_rep > GD_MAX_REP) return fail(GD_E_INVALID, "n_rep = %d", n_rep);
-  int per = (n_rep + n - 1) / n;  // prepair.C:366-375, maximising balance
+  int per = (n_rep + n - 1) / n;
   const McPara &mp = ch->mcpara;
   const bool exch = mp.steps_per_exchange > 0 && ch->size.n_tmp > 1;
   if (exch && n > 1) {
-    // exchange partners share (protein conf, ligand conf): cut at protein-conformation blocks
     const int block = ch->size.n_tmp * ch->size.n_lig;
     per = ((ch->size.n_prt + n - 1) / n) * block;
   }
   const int n_active = (n_rep + per - 1) / per;
   if (n_active < n) return fail(GD_E_INVALID, "%d replicas cannot keep %d GPUs busy", n_rep, n);
+  *per_out = per;
+  return GD_OK;
+}
+
+int SetParaT(Complex *ch, ParaT **pt)
+{
+  if (!ch || !pt) return fail(GD_E_INVALID, "null argument");
+  const int n = ngpu();
+  const int n_rep = ch->size.n_rep;
+  int per = 0;
+  GD_TRY(split_per_gpu(ch, n, &per));
   for (int g = 0; g < n; ++g) {
     pt[g]->rep_begin = per * g;
     pt[g]->rep_end = std::min(pt[g]->rep_begin + per, n_rep) - 1;
     pt[g]->n_rep = pt[g]->rep_end - pt[g]->rep_begin + 1;
     pt[g]->record_sz = (int)sizeof(Record) * pt[g]->n_rep;
   }
+  return GD_OK;
+}
+
+int gd_replica_range(const Complex *ch, int ngpu, int g, int *rep_begin, int *rep_end)
+{
+  if (!ch || !rep_begin || !rep_end) return fail(GD_E_INVALID, "null argument");
+  if (g < 0 || g >= ngpu) return fail(GD_E_INVALID, "GPU %d of %d", g, ngpu);
+  int per = 0;
+  GD_TRY(split_per_gpu(ch, ngpu, &per));
+  *rep_begin = per * g;
+  *rep_end = std::min(*rep_begin + per, ch->size.n_rep) - 1;
+  return GD_OK;
+}
+
+int gd_ensemble_create_complex_range(const Complex *cx, int rep_begin, int rep_end, uint64_t seed, int device,
+                                     gd_ensemble_t **out)
+{
+  if (!out || !cx) return fail(GD_E_INVALID, "null argument");
+  *out = nullptr;
+  if (rep_begin < 0 || rep_end < rep_begin || rep_end >= cx->size.n_rep)
+    return fail(GD_E_INVALID, "replica range [%d, %d] of %d", rep_begin, rep_end, cx->size.n_rep);
+  gd_ensemble *e = nullptr;
+  GD_TRY(ensemble_from_complex_range(cx, rep_begin, rep_end, seed, nullptr, device, &e));
+  *out = e;
   return GD_OK;
 }
 

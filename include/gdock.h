@@ -179,6 +179,15 @@ int gd_ensemble_create(const gd_pocket_desc_t *pockets, int npocket, const gd_jo
 /* The same from reference-layout Complexes (one job each; identical proteins share a pocket). */
 int gd_ensemble_create_complex(const Complex *const *cx, int n, const uint64_t *seeds, int device,
                                gd_ensemble_t **out);
+/* One process per GPU: replica range [*rep_begin, *rep_end] of GPU g of ngpu
+ * under SetParaT's split (exchange-aligned when exchange is on), and an
+ * ensemble of just that range of a Complex.  Philox counters use the global
+ * replica index, so with one seed on every GPU each replica's trajectory is
+ * the same whatever the number of GPUs.  No counterpart in the reference
+ * (its Dock drives every GPU from one process). */
+int gd_replica_range(const Complex *ch, int ngpu, int g, int *rep_begin, int *rep_end);
+int gd_ensemble_create_complex_range(const Complex *cx, int rep_begin, int rep_end, uint64_t seed, int device,
+                                     gd_ensemble_t **out);
 /* Initial energies (no move, forced accept). */
 int gd_ensemble_init(gd_ensemble_t *e);
 /* Advance every replica by nsteps MC steps, with a replica-exchange sweep

@@ -261,3 +261,20 @@ def test_dock_reuses_device_state(lib, enepara):
         check(lib.gd_set_option(b"dock_cache", 1))
     for a, b in zip(out[1], out[0]):
         assert a == b
+
+
+def test_sharded_run_equals_single(lib, enepara):
+    """The replicas of a Complex split over 3 shards (the split ranks use), run
+    one after another with one seed, equal the run of all replicas at once."""
+    from geauxdock_b200 import shard
+
+    rng = np.random.default_rng(23)
+    pk = synth.make_pocket(rng, 260, 3)
+    job = synth.make_job(rng, pk, 16, 2, 80, 4, synth.ladder(4, 0.3, 3.0), seed=1)
+    cx = synth.to_complex(job, pk, enepara, steps_per_exchange=10)
+    n = int(cx[0]["size"]["n_rep"])
+    whole = shard.run_shard(cx, 60, 10, 9, 0, 1)
+    parts = np.concatenate([shard.run_shard(cx, 60, 10, 9, r, 3) for r in range(3)])
+    assert len(whole) == len(parts) == n
+    for f in whole.dtype.names:
+        assert whole[f].tobytes() == parts[f].tobytes(), f

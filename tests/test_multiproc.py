@@ -56,3 +56,56 @@ def test_gloo_shards_cover_replicas(world):
     assert spans[0][0] == 0 and spans[-1][1] == 3520
     assert all(spans[i][1] == spans[i + 1][0] for i in range(len(spans) - 1))
     assert np.isclose(sum(n for _, _, n in shards), 3520)
+
+
+def _shard_worker(rank, world, port, q):
+    from geauxdock_b200 import params, shard, synth
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ep = params.optimize_enepara(params.default_enepara0())
+        rng = np.random.default_rng(3)
+        pk = synth.make_pocket(rng, 200, 4)
+        job = synth.make_job(rng, pk, 10, 3, 50, 3, synth.ladder(4, 0.3, 3.0), seed=1)
+        cx = synth.to_complex(job, pk, ep, steps_per_exchange=10)
+        b, e = shard.replica_range(cx, world, rank)
+        local = cx[0]["replica"][b:e].copy()
+        local["step"] = rank                     # mark who sent it
+        full = shard.gather_replicas(local)
+        if rank == 0:
+            q.put((b, e, full.tobytes(), cx[0]["replica"][:int(cx[0]["size"]["n_rep"])].tobytes()))
+        else:
+            q.put((b, e, None, None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2])
+def test_gloo_replica_shards_and_gather(world):
+    """Each rank's replica range (SetParaT's exchange-aligned split) and the
+    gather of the ranks' final states to rank 0, in replica order."""
+    from geauxdock_b200 import layout as Lo
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = [q.get(timeout=10) for _ in range(world)]
+    spans = sorted((b, e) for b, e, _, _ in got)
+    block = 4 * 3                                    # n_tmp * n_lig: one protein-conformation block
+    assert spans[0][0] == 0 and all(spans[i][1] == spans[i + 1][0] for i in range(world - 1))
+    assert all(b % block == 0 for b, _ in spans)
+    full, want = next((f, w) for _, _, f, w in got if f is not None)
+    full = np.frombuffer(full, dtype=Lo.REPLICA)
+    want = np.frombuffer(want, dtype=Lo.REPLICA)
+    assert spans[-1][1] == len(want) == len(full)
+    for (b, e), r in zip(spans, range(world)):
+        assert np.all(full["step"][b:e] == r)
+        assert np.array_equal(full["movematrix"][b:e], want["movematrix"][b:e])
+        assert np.array_equal(full["idx_rep"][b:e], want["idx_rep"][b:e])
