@@ -39,7 +39,7 @@ EXPORTED = [
     "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy", "gd_ensemble_eval_poses",
-    "gd_replica_range", "gd_ensemble_create_complex_range",
+    "gd_replica_range", "gd_ensemble_create_complex_range", "gd_load_complex",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
     "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
     "gd_server_config_default", "gd_server_create", "gd_server_submit", "gd_server_poll", "gd_server_drain",
@@ -81,6 +81,17 @@ class ServerStats(C.Structure):
         ("used_bytes", C.c_ulonglong), ("peak_bytes", C.c_ulonglong),
         ("warps_per_cta", C.c_int), ("grid", C.c_int), ("max_active_replicas", C.c_int),
         ("pocket_staged", C.c_int),
+    ]
+
+
+class LoadArgs(C.Structure):
+    """gd_load_args_t."""
+    _fields_ = [
+        ("lig_sdf", C.c_char_p), ("lhm_ff", C.c_char_p), ("prt_pdb", C.c_char_p), ("ligand_id", C.c_char_p),
+        ("molid", C.c_char_p), ("enepara0", C.c_void_p), ("enepara", C.c_void_p), ("num_temp", C.c_int),
+        ("floor_temp", C.c_float), ("ceiling_temp", C.c_float), ("translation_step", C.c_float),
+        ("rotation_step", C.c_float), ("steps_total", C.c_int), ("steps_per_dump", C.c_int),
+        ("steps_per_exchange", C.c_int),
     ]
 
 
@@ -144,6 +155,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_destroy": (i, [vp]), "gd_layout": (ll, [C.c_char_p]),
         "gd_ensemble_eval_poses": (i, [vp, i, i, vp, vp, i, vp, vp, vp]),
         "gd_replica_range": (i, [vp, i, i, ip, ip]),
+        "gd_load_complex": (i, [vp, vp]),
         "gd_ensemble_create_complex_range": (i, [vp, i, i, C.c_uint64, i, vp]),
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),

@@ -1317,6 +1317,7 @@ extern "C" long long gd_layout(const char *what)
   GD_L("sizeof.gd_request_t", sizeof(gd_request_t))
   GD_L("sizeof.gd_result_t", sizeof(gd_result_t))
   GD_L("sizeof.gd_server_stats_t", sizeof(gd_server_stats_t))
+  GD_L("sizeof.gd_load_args_t", sizeof(gd_load_args_t))
   GD_L("gd_server_stats_t.warps_per_cta", offsetof(gd_server_stats_t, warps_per_cta))
   GD_L("gd_result_t.t_done", offsetof(gd_result_t, t_done))
 #undef GD_L

@@ -285,6 +285,30 @@ int gd_server_get_stats(gd_server_t *s, gd_server_stats_t *out);
 /* Stops the loop; requests not finished yet are cancelled. */
 int gd_server_destroy(gd_server_t *s);
 
+/* ---------------------------------------------------------------- loaders
+ * The reference frontend's input path for one job (src/frontend/load.C
+ * loadLigand / loadLHM / loadProtein, util_optimize_soa.C Optimize*, util.C
+ * SetPocketCenter / SetTemperature / SetReplica): ligand .sdf with its
+ * conformer ensemble (conformers within 0.1 A RMSD of the native pose after
+ * superposition dropped), the .ff file's KDE points, pocket-specific
+ * potential and MCS rows of `ligand_id`, and the protein .pdb's
+ * ENDMDL-terminated models, into a Complex laid out as the GPU frontend
+ * builds it.  The force field comes from the caller (parameter files parsed
+ * elsewhere; gd_optimize_enepara for the tables).  Returns n_rep or a
+ * negative status. */
+typedef struct gd_load_args {
+  const char *lig_sdf, *lhm_ff, *prt_pdb;
+  const char *ligand_id;        /* MCS rows of this ligand in the .ff file */
+  const char *molid;            /* SDF data tag naming the molecule ("MOLID") */
+  const EnePara0 *enepara0;     /* raw parameters (point ele/hpp tables) */
+  const EnePara *enepara;       /* precomputed tables copied into the Complex */
+  int num_temp;
+  float floor_temp, ceiling_temp;
+  float translation_step, rotation_step;
+  int steps_total, steps_per_dump, steps_per_exchange;
+} gd_load_args_t;
+int gd_load_complex(const gd_load_args_t *args, Complex *out);
+
 /* Measured FP32 FMA throughput of the current GPU (TFLOP/s, 2 flops per FMA):
  * the denominator of the pair kernel's roofline. */
 int gd_fp32_peak(double *tflops);

@@ -24,6 +24,8 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <omp.h>
@@ -38,16 +40,75 @@
 // The reference backend: defines Dock() and the static MonteCarlo_d().
 #include <backend_cpu_mic.C>
 
-// loadLigand calls the Fortran Kabsch routine u3b_ (src/frontend/rmsd.f) only
-// to drop near-duplicate conformers (src/frontend/load.C:421-428).  gfortran is
-// absent; this stand-in reports a large RMSD so that every conformer is kept.
-// It does not affect conformer 0 (the native pose), which is the one the
-// known-answer line reports.
-extern "C" void u3b_(float (*)[MAXLIG], float (*)[MAXLIG][3], float (*)[MAXLIG][3], int *n, int *mode,
+// loadLigand calls the Fortran superposition routine u3b_ (src/frontend/rmsd.f,
+// Kabsch's algorithm) only to drop near-duplicate conformers
+// (src/frontend/load.C:421-428); gfortran is absent, so this restates what it
+// returns there: *rms = the weighted sum of squared deviations after the
+// optimal rotation and translation of x onto y.  Kabsch (Acta Cryst. A32, 922
+// (1976); A34, 827 (1978)): with the weighted centred correlation R = sum w a b^T,
+// E = sum w (|a|^2 + |b|^2) - 2 (s1 + s2 + sign(det R) s3), s_i the singular
+// values of R (square roots of the eigenvalues of R^T R, here by Jacobi
+// rotations).  u and t are left as the identity and zero (the caller reads
+// only rms).
+extern "C" void u3b_(float (*w)[MAXLIG], float (*x)[MAXLIG][3], float (*y)[MAXLIG][3], int *n, int *mode,
                      float *rms, float (*u)[3][3], float (*t)[3], int *ier)
 {
   (void)mode;
-  *rms = 1.0e6f * (float)(*n);
+  const int m = *n;
+  double W = 0, xc[3] = {0, 0, 0}, yc[3] = {0, 0, 0};
+  for (int i = 0; i < m; ++i) {
+    W += (*w)[i];
+    for (int k = 0; k < 3; ++k) {
+      xc[k] += (*w)[i] * (*x)[i][k];
+      yc[k] += (*w)[i] * (*y)[i][k];
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    xc[k] /= W;
+    yc[k] /= W;
+  }
+  double R[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e0 = 0;
+  for (int i = 0; i < m; ++i) {
+    double a[3], b[3];
+    for (int k = 0; k < 3; ++k) {
+      a[k] = (*x)[i][k] - xc[k];
+      b[k] = (*y)[i][k] - yc[k];
+      e0 += (*w)[i] * (a[k] * a[k] + b[k] * b[k]);
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) R[r][c] += (*w)[i] * a[r] * b[c];
+  }
+  const double det = R[0][0] * (R[1][1] * R[2][2] - R[1][2] * R[2][1]) -
+                     R[0][1] * (R[1][0] * R[2][2] - R[1][2] * R[2][0]) +
+                     R[0][2] * (R[1][0] * R[2][1] - R[1][1] * R[2][0]);
+  double M[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) M[r][c] = R[0][r] * R[0][c] + R[1][r] * R[1][c] + R[2][r] * R[2][c];
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    const double off = M[0][1] * M[0][1] + M[0][2] * M[0][2] + M[1][2] * M[1][2];
+    if (off < 1e-300) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (M[p][q] == 0.0) continue;
+        const double th = 0.5 * std::atan2(2.0 * M[p][q], M[q][q] - M[p][p]);
+        const double c = std::cos(th), s = std::sin(th);
+        for (int k = 0; k < 3; ++k) {
+          const double kp = M[k][p], kq = M[k][q];
+          M[k][p] = c * kp - s * kq;
+          M[k][q] = s * kp + c * kq;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double pk = M[p][k], qk = M[q][k];
+          M[p][k] = c * pk - s * qk;
+          M[q][k] = s * pk + c * qk;
+        }
+      }
+  }
+  double sv[3] = {std::sqrt(std::max(M[0][0], 0.0)), std::sqrt(std::max(M[1][1], 0.0)),
+                  std::sqrt(std::max(M[2][2], 0.0))};
+  std::sort(sv, sv + 3);
+  const double e = e0 - 2.0 * (sv[2] + sv[1] + (det < 0 ? -sv[0] : sv[0]));
+  *rms = (float)std::max(e, 0.0);
   for (int i = 0; i < 3; ++i) {
     for (int j = 0; j < 3; ++j) (*u)[i][j] = (i == j) ? 1.0f : 0.0f;
     (*t)[i] = 0.0f;
