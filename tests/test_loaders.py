@@ -122,3 +122,16 @@ def test_loader_errors_are_status_codes(lib, tmp_path):
     with pytest.raises(GdockError) as ei:
         loaders.load_complex(lig / "1a07C1.sdf", lig / "1a07C1-0.8.ff", bad, "1a07C1", e0)
     assert ei.value.code == GD_E_INVALID
+
+
+def test_known_answer_through_loader(oracle_lib):
+    """The reference's known-answer line (doc/instructions.txt:186-187) from a
+    Complex built by this loader: initial energies of replica 0 of 1a07C1 x
+    1a07C-1, FP64 oracle rounded as the reference prints them."""
+    from test_oracle import _known_answer_line
+
+    lig = DATA / "astex" / "ligands"
+    cx = _ours("1a07C1", lig / "1a07C1.sdf", lig / "1a07C1-0.8.ff", DATA / "astex" / "proteins" / "1a07C-1.pdb",
+               num_temp=1)
+    e, _ = oracle_lib.energy(cx, 0, 0, np.zeros(6, np.float32))
+    assert [round(float(v), 4) for v in e] == pytest.approx(_known_answer_line(), abs=1e-12)
