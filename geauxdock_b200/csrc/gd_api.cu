@@ -26,6 +26,8 @@ struct Options {
   int graph = 1;  // replay whole exchange intervals from a captured graph
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
+  long long wait_limit = 0;   // polls of a bounded shared-memory wait (0: the kernel's default)
+  int stall_test = 0;         // test hook: staging barriers that never complete (bounded waits run out)
 };
 Options g_opt;
 int g_ngpu = -1;
@@ -95,6 +97,7 @@ struct gd_ensemble {
   // timing of the Monte Carlo launches
   std::vector<cudaEvent_t> ev;
   int ev_used = 0;
+  uint32_t wait_limit = 0, stall_bytes = 0;  // bounded-wait limit and the test hook (options)
   int launches = 0;      // Monte Carlo kernel launches (or graph replays of one)
   int all_launches = 0;  // every kernel of this library launched on the stream
 };
@@ -269,6 +272,8 @@ int finish_create(gd_ensemble *e)
   e->kernel = o.kernel;
   e->precision = o.precision;
   e->use_graph = o.graph != 0;
+  e->wait_limit = (uint32_t)o.wait_limit;
+  e->stall_bytes = o.stall_test ? 16u : 0u;
   TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab, o.stage != 0 ? 1 : 0};
   if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
   if (o.warps > 0) return configure(e, tc);
@@ -337,6 +342,8 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
   a.P = e->tc.stage ? e->Pmax : 0;
   a.Kst = e->Kst;
   a.lig_slots = e->lig_slots;
+  a.wait_limit = e->wait_limit;
+  a.stall_bytes = e->stall_bytes;
   return a;
 }
 
@@ -589,6 +596,12 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "dock_cache") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_cache = %lld", v);
     g_opt.dock_cache = (int)v;
+  } else if (n == "wait_limit") {
+    if (v < 0 || v > 0xffffffffLL) return fail(GD_E_INVALID, "wait_limit = %lld", v);
+    g_opt.wait_limit = v;
+  } else if (n == "stall_test") {
+    if (v != 0 && v != 1) return fail(GD_E_INVALID, "stall_test = %lld", v);
+    g_opt.stall_test = (int)v;
   } else if (n == "graph") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "graph = %lld", v);
     g_opt.graph = (int)v;
@@ -611,6 +624,8 @@ long long gd_get_option(const char *name)
   if (n == "graph") return g_opt.graph;
   if (n == "stage") return g_opt.stage;
   if (n == "dock_cache") return g_opt.dock_cache;
+  if (n == "wait_limit") return g_opt.wait_limit;
+  if (n == "stall_test") return g_opt.stall_test;
   return GD_E_INVALID;
 }
 

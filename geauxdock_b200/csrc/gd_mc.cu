@@ -704,7 +704,7 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
     fence_proxy_async_smem();
     uint32_t bytes = (uint32_t)sizeof(DevParams) + (pocket_in_smem ? 24u * (uint32_t)P : 0u);
     if (kde_in_smem) bytes += 16u * (uint32_t)J.nkde;
-    mbar_expect_tx(bar, bytes);
+    mbar_expect_tx(bar, bytes + A.stall_bytes);
     bulk_g2s(smem + sl.params, J.par, (uint32_t)sizeof(DevParams), bar);
     if (pocket_in_smem) {
       bulk_g2s(smem + sl.pos, J.pos + (size_t)wi.prt * P, 16u * (uint32_t)P, bar);
@@ -714,7 +714,7 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
   }
   int2 *lg = reinterpret_cast<int2 *>(smem + sl.lgrp);
   for (int a = threadIdx.x; a < J.natom; a += blockDim.x) lg[a] = J.lgrp[a];
-  const bool ok = mbar_wait(bar, phase, kWaitLimit);
+  const bool ok = mbar_wait(bar, phase, A.wait_limit ? A.wait_limit : kWaitLimit);
   phase ^= 1u;
   return ok;
 }
@@ -752,7 +752,9 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     if (wi.job != prev_job || wi.prt != prev_prt) {
       if (!stage_item<PREC == kFP64>(A, J, wi, smem, sl, &bar, phase)) {
         if (threadIdx.x == 0) atomicOr(A.err, kErrTimeout);
-        mbar_wait(&bar, phase ^ 1u, kWaitLimit);  // let the copies in flight land before exiting
+        // the copies it issued complete whatever the barrier's count says; wait
+        // (bounded) for the phase once more before the CTA's shared memory goes
+        mbar_wait(&bar, phase ^ 1u, A.wait_limit ? A.wait_limit : kWaitLimit);
         return;
       }
       prev_job = wi.job;

@@ -278,3 +278,31 @@ def test_sharded_run_equals_single(lib, enepara):
     assert len(whole) == len(parts) == n
     for f in whole.dtype.names:
         assert whole[f].tobytes() == parts[f].tobytes(), f
+
+
+def test_bounded_wait_reports_timeout(lib, enepara):
+    """A staging barrier that never completes (the stall_test hook announces
+    bytes no copy delivers) makes the kernel's bounded wait give up: the host
+    gets GD_E_TIMEOUT, and the CUDA context runs the next ensemble normally."""
+    from geauxdock_b200._lib import GD_E_TIMEOUT
+
+    cx = _small_ensemble(enepara, seed=12)
+    try:
+        check(lib.gd_set_option(b"wait_limit", 4096))
+        check(lib.gd_set_option(b"stall_test", 1))
+        ens = dock.Ensemble.from_complexes([cx], [1])
+        try:
+            ens.init()
+            with pytest.raises(GdockError) as ei:
+                ens.sync()
+            assert ei.value.code == GD_E_TIMEOUT
+        finally:
+            ens.close()
+    finally:
+        check(lib.gd_set_option(b"stall_test", 0))
+        check(lib.gd_set_option(b"wait_limit", 0))
+    with dock.Ensemble.from_complexes([cx], [1]) as ens:
+        ens.init()
+        ens.run(20, 10)
+        ens.sync()
+        assert np.isfinite(ens.replicas(0)["energy"][:int(cx[0]["size"]["n_rep"])]).all()
