@@ -39,7 +39,8 @@ EXPORTED = [
     "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy", "gd_ensemble_eval_poses",
-    "gd_replica_range", "gd_ensemble_create_complex_range", "gd_load_complex",
+    "gd_replica_range", "gd_ensemble_create_complex_range", "gd_load_complex", "gd_ensemble_cluster",
+    "gd_ensemble_best_poses",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
     "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
     "gd_server_config_default", "gd_server_create", "gd_server_submit", "gd_server_poll", "gd_server_drain",
@@ -92,6 +93,14 @@ class LoadArgs(C.Structure):
         ("floor_temp", C.c_float), ("ceiling_temp", C.c_float), ("translation_step", C.c_float),
         ("rotation_step", C.c_float), ("steps_total", C.c_int), ("steps_per_dump", C.c_int),
         ("steps_per_exchange", C.c_int),
+    ]
+
+
+class Cluster(C.Structure):
+    """gd_cluster_t."""
+    _fields_ = [
+        ("representative", C.c_int), ("size", C.c_int), ("relative_size", C.c_float), ("z_score", C.c_float),
+        ("rep_energy", C.c_float), ("mean_energy", C.c_float), ("rep_rmsd", C.c_float), ("pad_", C.c_int),
     ]
 
 
@@ -156,6 +165,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_ensemble_eval_poses": (i, [vp, i, i, vp, vp, i, vp, vp, vp]),
         "gd_replica_range": (i, [vp, i, i, ip, ip]),
         "gd_load_complex": (i, [vp, vp]),
+        "gd_ensemble_cluster": (i, [vp, i, i, vp, C.c_float, vp, i, ip, vp, vp]),
+        "gd_ensemble_best_poses": (i, [vp, i, vp, vp]),
         "gd_ensemble_create_complex_range": (i, [vp, i, i, C.c_uint64, i, vp]),
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),

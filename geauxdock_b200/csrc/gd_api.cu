@@ -1139,6 +1139,34 @@ int gd_ensemble_replicas(gd_ensemble_t *e, int job, ReplicaMC *out)
   return GD_OK;
 }
 
+int gd_ensemble_best_poses(gd_ensemble_t *e, int job, float *best_mm, double *best_energy)
+{
+  if (!e || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  GD_TRY(set_device(e->device));
+  const DevJob &J = e->jobs[job].dj;
+  std::vector<RepStats> s(J.nrep);
+  GD_CUDA(cudaMemcpyAsync(s.data(), J.stats, sizeof(RepStats) * s.size(), cudaMemcpyDeviceToHost, e->st));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  for (int r = 0; r < J.nrep; ++r) {
+    if (best_mm)
+      for (int k = 0; k < 6; ++k) best_mm[6 * (size_t)r + k] = s[r].best_mm[k];
+    if (best_energy) best_energy[r] = s[r].best_e;
+  }
+  return GD_OK;
+}
+
+int gd_ensemble_cluster(gd_ensemble_t *e, int job, int ref_lig, const float *ref_mm, float rmsd_cut,
+                        gd_cluster_t *clusters, int max_clusters, int *n_clusters, int *cluster_of,
+                        float *rmsd_to_ref)
+{
+  if (!e || job < 0 || job >= (int)e->jobs.size()) return fail(GD_E_INVALID, "job %d", job);
+  if (!n_clusters || (max_clusters > 0 && !clusters) || max_clusters < 0) return fail(GD_E_INVALID, "null argument");
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  return cluster_job(e->jobs[job].dj, e->d_jobs + job, e->st, ref_lig, ref_mm, rmsd_cut, clusters, max_clusters,
+                     n_clusters, cluster_of, rmsd_to_ref);
+}
+
 int gd_ensemble_eval_poses(gd_ensemble_t *e, int job, int n, const int *conf, const float *mm, int precision,
                            float *out, double *out64, float *raw)
 {
@@ -1333,6 +1361,7 @@ extern "C" long long gd_layout(const char *what)
   GD_L("sizeof.gd_result_t", sizeof(gd_result_t))
   GD_L("sizeof.gd_server_stats_t", sizeof(gd_server_stats_t))
   GD_L("sizeof.gd_load_args_t", sizeof(gd_load_args_t))
+  GD_L("sizeof.gd_cluster_t", sizeof(gd_cluster_t))
   GD_L("gd_server_stats_t.warps_per_cta", offsetof(gd_server_stats_t, warps_per_cta))
   GD_L("gd_result_t.t_done", offsetof(gd_result_t, t_done))
 #undef GD_L

@@ -111,6 +111,11 @@ int pack_job(const JobData &jd, const DevPocket &pk, const EnePara &ep, bool wan
              DevJobBuf &out, const DevJobBuf *reuse = nullptr, cudaStream_t st = nullptr);
 // Stream-ordered variant (cudaMallocAsync + a copy on `st`), no records.
 int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cudaStream_t st, DevJobBuf &out);
+// Best poses of a job's replicas, their RMSD to a reference pose and their
+// leader clustering in energy order (gd_analysis.cu).
+int cluster_job(const DevJob &J, const DevJob *d_job, cudaStream_t st, int ref_lig, const float ref_mm[6],
+                float rmsd_cut, gd_cluster_t *clusters, int max_clusters, int *n_clusters, int *cluster_of,
+                float *rmsd_to_ref);
 void free_pocket(DevPocket &p);
 void free_job(DevJobBuf &j);
 void free_job_async(DevJobBuf &j, cudaStream_t st);

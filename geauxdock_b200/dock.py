@@ -155,6 +155,30 @@ class Ensemble:
                                               None if raw is None else raw.ctypes.data))
         return out, raw, out64
 
+    def best_poses(self, job: int = 0):
+        """Each replica's best pose: (movematrix [nrep, 6] float32, total energy [nrep] float64)."""
+        n = check(self.lib.gd_ensemble_num_replicas(self.h, job))
+        mm = np.zeros((n, 6), np.float32)
+        e = np.zeros(n, np.float64)
+        check(self.lib.gd_ensemble_best_poses(self.h, job, mm.ctypes.data, e.ctypes.data))
+        return mm, e
+
+    def cluster(self, job: int = 0, rmsd_cut: float = 2.0, ref_lig: int = 0, ref_mm=None, max_clusters: int = 4096):
+        """Best pose per replica, RMSD to the reference pose (default: the native pose) and leader
+        clustering in energy order: (list of cluster dicts, cluster_of [nrep], rmsd_to_ref [nrep])."""
+        from ._lib import Cluster
+
+        n = check(self.lib.gd_ensemble_num_replicas(self.h, job))
+        out = (Cluster * max_clusters)()
+        ncl = C.c_int()
+        cof = np.zeros(n, np.int32)
+        rmsd = np.zeros(n, np.float32)
+        mm = None if ref_mm is None else np.ascontiguousarray(ref_mm, np.float32)
+        check(self.lib.gd_ensemble_cluster(self.h, job, ref_lig, None if mm is None else mm.ctypes.data, rmsd_cut,
+                                           out, max_clusters, C.byref(ncl), cof.ctypes.data, rmsd.ctypes.data))
+        cl = [{k: getattr(c, k) for k, _ in Cluster._fields_ if k != "pad_"} for c in out[:min(ncl.value, max_clusters)]]
+        return cl, cof, rmsd
+
     def autotune(self, steps: int = 4) -> str:
         buf = C.create_string_buffer(8192)
         check(self.lib.gd_ensemble_autotune(self.h, steps, buf, len(buf)))

@@ -214,6 +214,30 @@ int gd_ensemble_stats(gd_ensemble_t *e, int job, double *out8);
  * the Complex caps.  Waits for the ensemble's stream first. */
 int gd_ensemble_eval_poses(gd_ensemble_t *e, int job, int n, const int *conf, const float *mm, int precision,
                            float *out, double *out64, float *raw);
+/* Post-analysis of job `job`: each replica's best pose (the lowest total
+ * energy it visited, from its FP64 statistics), the pose's RMSD to a
+ * reference pose (ligand conformation ref_lig at movematrix ref_mm; NULL: the
+ * native pose, conformation 0 at zero), and the best poses clustered in
+ * order of energy: a pose joins the first cluster whose lowest-energy pose is
+ * within rmsd_cut (A), else it starts one.  Up to max_clusters summaries go
+ * to `clusters` (all are counted in *n_clusters); cluster_of[nrep] and
+ * rmsd_to_ref[nrep] (may be NULL) per replica.  No counterpart in the
+ * reference (src/analysis/record.h:50-59 sketches the medoid summary). */
+typedef struct gd_cluster {
+  int representative;   /* replica whose best pose has the lowest energy in the cluster */
+  int size;             /* best poses in the cluster */
+  float relative_size;  /* size / replicas */
+  float z_score;        /* (representative energy - mean best energy) / standard deviation */
+  float rep_energy;     /* total energy of the representative */
+  float mean_energy;    /* mean total energy of the members */
+  float rep_rmsd;       /* RMSD of the representative to the reference pose, A */
+  int pad_;
+} gd_cluster_t;
+/* Each replica's best pose: movematrix [nrep][6] and total energy [nrep] (FP64). */
+int gd_ensemble_best_poses(gd_ensemble_t *e, int job, float *best_mm, double *best_energy);
+int gd_ensemble_cluster(gd_ensemble_t *e, int job, int ref_lig, const float *ref_mm, float rmsd_cut,
+                        gd_cluster_t *clusters, int max_clusters, int *n_clusters, int *cluster_of,
+                        float *rmsd_to_ref);
 /* Choose the tile shape (replicas per CTA, pair tile, pocket staging) by timing
  * candidates on a snapshot of the state (restored after each).  steps: MC
  * steps per launch to tune for (the chunk the caller runs, e.g. its exchange

@@ -77,10 +77,10 @@ def test_ctypes_mirrors_of_api_structs(lib):
     """The ctypes structures of the serving and descriptor API match the C layout."""
     import ctypes as C
 
-    from geauxdock_b200._lib import (JobDesc, LoadArgs, PocketDesc, Request, Result, ServerConfig, ServerStats,
-                                     layout)
+    from geauxdock_b200._lib import (Cluster, JobDesc, LoadArgs, PocketDesc, Request, Result, ServerConfig,
+                                     ServerStats, layout)
 
-    for name, cls in (("gd_job_desc_t", JobDesc), ("gd_pocket_desc_t", PocketDesc), ("gd_load_args_t", LoadArgs),
+    for name, cls in (("gd_job_desc_t", JobDesc), ("gd_pocket_desc_t", PocketDesc), ("gd_load_args_t", LoadArgs), ("gd_cluster_t", Cluster),
                       ("gd_server_config_t", ServerConfig), ("gd_request_t", Request),
                       ("gd_result_t", Result), ("gd_server_stats_t", ServerStats)):
         assert layout(f"sizeof.{name}") == C.sizeof(cls), name
