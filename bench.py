@@ -79,6 +79,9 @@ def _args():
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     p.add_argument("--serve-steps", type=int, default=2000)
+    p.add_argument("--serve-max-active", type=int, default=0,
+                   help="replicas per serving round (0: the server's default, four waves of resident replicas)")
+    p.add_argument("--serve-round", type=int, default=STEPS_PER_INTERVAL, help="MC steps per serving round")
     return p.parse_args()
 
 
@@ -336,7 +339,8 @@ def run_serving(args, local: int) -> dict:
                 "mean_queue_s": float(np.mean([r["t_admit"] - r["t_submit"] for r in res])),
                 "value": evals / span, "unit": UNIT, "req_per_s": len(batch) / span, "span_s": span}
 
-    with dock.Server(pockets, ep, device=local, max_atoms=80) as srv:
+    with dock.Server(pockets, ep, device=local, max_atoms=80, max_active_replicas=args.serve_max_active,
+                     steps_per_round=args.serve_round) as srv:
         srv.submit(jobs[-1], 100, STEPS_PER_INTERVAL, results=False)   # warm-up
         srv.submit(jobs[-2], 100, STEPS_PER_INTERVAL, results=False)
         srv.drain(900_000)

@@ -470,7 +470,9 @@ int server_configure(gd_server *s)
   s->Kst = best_kst;
   s->smem = best_smem;
   s->grid = best_occ * nsm;
-  if (s->cfg.max_active_replicas <= 0) s->cfg.max_active_replicas = 2 * best_occ * nsm * best_w;
+  // four waves of resident replica-warps per round: more balanced rounds (items
+  // of uneven jobs) than two, with the same latency below saturation
+  if (s->cfg.max_active_replicas <= 0) s->cfg.max_active_replicas = 4 * best_occ * nsm * best_w;
   return GD_OK;
 }
 

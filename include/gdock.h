@@ -261,7 +261,7 @@ typedef struct gd_server gd_server_t;
 
 typedef struct gd_server_config {
   unsigned long long hbm_budget_bytes; /* device bytes of admitted jobs (default 100 GB) */
-  int max_active_replicas;  /* replicas in one round (0: two waves of resident replica-warps) */
+  int max_active_replicas;  /* replicas in one round (0: four waves of resident replica-warps) */
   int max_jobs;             /* admitted jobs at a time (result staging slots), default 256 */
   int max_replicas_per_job; /* default 1024 */
   int max_atoms;            /* largest ligand accepted (sizes the per-warp buffers), default 128 */
