@@ -501,6 +501,7 @@ def run_ours(args) -> None:
     rec_h = np.frombuffer(rec_pin.numpy(), dtype=Lo.RECORD, count=n_rep)
     e2e_calls = 5
     e2e_times = []
+    check(lib.gd_set_option(b"device_base", local))   # this rank's GPU for the drop-in API
     with dock.DockSession(1, seed=77 + rank) as s:
         s.dock(cx_h, rec_h)              # warm-up (also the first-use cost of the library)
         barrier()

@@ -26,6 +26,7 @@ struct Options {
   int graph = 1;  // replay whole exchange intervals from a captured graph
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
+  int device_base = 0;        // the drop-in API's GPU g is CUDA device device_base + g
   long long wait_limit = 0;   // polls of a bounded shared-memory wait (0: the kernel's default)
   int stall_test = 0;         // test hook: staging barriers that never complete (bounded waits run out)
 };
@@ -105,6 +106,9 @@ struct gd_ensemble {
 namespace {
 
 int set_device(int d) { GD_CUDA(cudaSetDevice(d)); return GD_OK; }
+
+// CUDA device of the drop-in API's GPU g.
+int dev_of(int g) { return opts().device_base + g; }
 
 // Work items: runs of consecutive replicas of one job with the same protein
 // conformation, at most `warps` long; heaviest (L x P) first.
@@ -596,6 +600,11 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "dock_cache") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_cache = %lld", v);
     g_opt.dock_cache = (int)v;
+  } else if (n == "device_base") {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) count = 0;
+    if (v < 0 || (count > 0 && v >= count)) return fail(GD_E_INVALID, "device_base = %lld (%d devices)", v, count);
+    g_opt.device_base = (int)v;
   } else if (n == "wait_limit") {
     if (v < 0 || v > 0xffffffffLL) return fail(GD_E_INVALID, "wait_limit = %lld", v);
     g_opt.wait_limit = v;
@@ -625,6 +634,7 @@ long long gd_get_option(const char *name)
   if (n == "stage") return g_opt.stage;
   if (n == "dock_cache") return g_opt.dock_cache;
   if (n == "wait_limit") return g_opt.wait_limit;
+  if (n == "device_base") return g_opt.device_base;
   if (n == "stall_test") return g_opt.stall_test;
   return GD_E_INVALID;
 }
@@ -635,9 +645,10 @@ int SetDevice(void)
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) return fail(GD_E_NODEVICE, "no CUDA device");
   const int n = ngpu();
-  if (n > count) return fail(GD_E_NODEVICE, "%d GPUs requested, %d present", n, count);
+  if (dev_of(n - 1) >= count)
+    return fail(GD_E_NODEVICE, "%d GPUs from device %d requested, %d present", n, dev_of(0), count);
   for (int g = 0; g < n; ++g) {
-    GD_CUDA(cudaSetDevice(g));
+    GD_CUDA(cudaSetDevice(dev_of(g)));
     GD_CUDA(cudaDeviceSetCacheConfig(cudaFuncCachePreferShared));  // prepair.C:11-20
   }
   return GD_OK;
@@ -648,7 +659,7 @@ int DeviceAlloc(Complex **cd, Record **rd, gd_rng_t **rng)
   if (!cd || !rd || !rng) return fail(GD_E_INVALID, "null argument");
   const int n = ngpu();
   for (int g = 0; g < n; ++g) {
-    GD_CUDA(cudaSetDevice(g));
+    GD_CUDA(cudaSetDevice(dev_of(g)));
     cd[g] = nullptr;
     rd[g] = nullptr;
     if (cudaMalloc((void **)&cd[g], sizeof(Complex)) != cudaSuccess)
@@ -665,7 +676,7 @@ int DeviceFree(Complex **cd, Record **rd, gd_rng_t **rng)
   if (!cd || !rd || !rng) return fail(GD_E_INVALID, "null argument");
   const int n = ngpu();
   for (int g = 0; g < n; ++g) {
-    GD_CUDA(cudaSetDevice(g));
+    GD_CUDA(cudaSetDevice(dev_of(g)));
     if (rng[g] && rng[g]->dock) destroy(rng[g]->dock);
     if (cd[g]) GD_CUDA(cudaFree(cd[g]));
     if (rd[g]) GD_CUDA(cudaFree(rd[g]));
@@ -743,7 +754,7 @@ int CopyH2D(Complex *ch, Complex **cd, ParaT **pt)
   if (!ch || !cd || !pt) return fail(GD_E_INVALID, "null argument");
   const int n = ngpu();
   for (int g = 0; g < n; ++g) {
-    GD_CUDA(cudaSetDevice(g));
+    GD_CUDA(cudaSetDevice(dev_of(g)));
     ch->rep_begin = pt[g]->rep_begin;  // prepair.C:119-123
     ch->rep_end = pt[g]->rep_end;
     GD_CUDA(cudaMemcpy(cd[g], ch, sizeof(Complex), cudaMemcpyHostToDevice));
@@ -797,24 +808,24 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
     }
     // each Dock call draws a fresh stream from the handle (the reference's curand state advances)
     const uint64_t seed = rng[g]->seed + (rng[g]->calls++ << 32);
-    rc = dock_ensemble(rng[g], ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], g, &ens[g]);
+    rc = dock_ensemble(rng[g], ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], dev_of(g), &ens[g]);
   }
   tr.mark("pack+create");
   // initial energy, backend_gpu.cu:87-91: one step, no move, forced accept
   for (int g = 0; g < n && rc == GD_OK; ++g) {
-    rc = set_device(g);
+    rc = set_device(dev_of(g));
     if (rc == GD_OK) rc = launch_mc(ens[g], 0, 1, kMcInitial | kMcRecord | kMcResetRecord | kMcStoreAccept);
   }
   tr.mark("initial (enqueued)");
   // dump chunks, backend_gpu.cu:96-114
   for (int s1 = 0; s1 < steps_total && rc == GD_OK; s1 += spd) {
     for (int g = 0; g < n && rc == GD_OK; ++g) {
-      rc = set_device(g);
+      rc = set_device(dev_of(g));
       ens[g]->step = s1;
       if (rc == GD_OK) rc = advance(ens[g], spd, spx, kMcResetRecord, kMcRecord, kMcStoreAccept);
     }
     for (int g = 0; g < n && rc == GD_OK; ++g) {
-      rc = set_device(g);
+      rc = set_device(dev_of(g));
       if (rc != GD_OK) break;
       const cudaError_t ce = cudaMemcpyAsync(rh + pt[g]->rep_begin, rd[g], sizeof(Record) * (size_t)pt[g]->n_rep,
                                              cudaMemcpyDeviceToHost, ens[g]->st);
@@ -830,7 +841,7 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
   }
   // final replica states: device Complex (as the reference) and the host Complex
   for (int g = 0; g < n && rc == GD_OK; ++g) {
-    rc = set_device(g);
+    rc = set_device(dev_of(g));
     if (rc != GD_OK) break;
     const DevJob &J = ens[g]->jobs[0].dj;
     const size_t bytes = sizeof(ReplicaMC) * (size_t)J.nrep;

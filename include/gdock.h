@@ -95,7 +95,9 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
  * large to stage are always read through L1), "dock_cache" (1: Dock keeps
  * its packed device state per GPU handle and refills it in place when the next
  * Complex has the same shapes, keeping the packed protein when its bytes are
- * unchanged; 0: everything is rebuilt and freed per call), "wait_limit"
+ * unchanged; 0: everything is rebuilt and freed per call), "device_base" (the
+ * drop-in API's GPU g is CUDA device device_base + g, for one process per GPU;
+ * set it before SetDevice/DeviceAlloc and keep it), "wait_limit"
  * (polls of the kernel's bounded shared-memory waits before they give up and
  * report GD_E_TIMEOUT; 0: the default), "stall_test" (test hook, 0 in normal
  * use: ensembles announce bytes to their staging barriers that no copy

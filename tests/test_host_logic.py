@@ -71,6 +71,9 @@ def test_options_validated(lib):
     assert lib.gd_get_option(b"graph") == 1
     assert lib.gd_get_option(b"stage") == -1
     assert lib.gd_get_option(b"dock_cache") == 1
+    assert lib.gd_get_option(b"device_base") == 0
+    with pytest.raises(GdockError):
+        check(lib.gd_set_option(b"device_base", -1))
     assert lib.gd_get_option(b"stall_test") == 0 and lib.gd_get_option(b"wait_limit") == 0
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"stall_test", 3))
