@@ -15,8 +15,14 @@ roofline   the batched Monte Carlo kernel against the measured FP32 FMA peak
 plain      the plain kernel (the reference's launch structure) on the same work
 cpu_baseline  the reference's own CPU Monte Carlo (built from its sources) on
            the box's host cores, a bounded sample of the same workload
+screening  512 ligands of 12-64 atoms (204,800 replicas) in one persistent
+           launch per exchange interval, against one plain launch per ligand
+serving    the request loop under Poisson arrivals at 200 req/s and at 70 % of
+           capacity: throughput, p50/p99 latency, against the plain kernel run
+           one request at a time (a bounded sample of the 10,000-request stream)
 
---impl reference runs the reference's CPU implementation instead (rank 0).
+--workload ensemble|screening|serving runs one leg.  --impl reference runs the
+reference's CPU implementation instead (rank 0).
 Multi-GPU (torchrun): each rank runs its own ensemble (weak scaling, no
 data-path collective); timing is the max over ranks.
 """

@@ -11,9 +11,11 @@
 //                        type): hydrophobic-contact points first, each part
 //                        sorted by point type, padded with inert points
 //   force-field tables   tab4[24][32] float4 (1/p1a, -p2a/p1a, -pmf0, pmf1) for the FP32 pair loop
-//                        tab2[24][32] float2 (scaled hdb1, hdb0), unused pairs zeroed
+//                        tab2[24][32] float2 (hdb1 c, -hdb0 hdb1 c), zero where hdb0 <= 0.1
 //                        ref4[24][32] float4 (p1a, p2a, hdb0, hdb1) as in EnePara (FP64, plain)
-//   ligand conformation  lig[L] float4 (x, y, z, charge), atoms grouped by type
+//   ligand conformation  lig[L] float4 (x, y, z, charge), atoms grouped by type; the
+//                        rotated pose of a replica lives in shared memory with
+//                        every value twice (packed f32x2 operands)
 //   KDE points           kde[K] float4 (x, y, z, type), sorted by type, with
 //                        per-type ranges
 //   MCS templates        mcs[L][M] float4 (x, y, z, valid), atom-major
@@ -38,9 +40,9 @@ constexpr int kPadType = 30;             // point type given to padding points
 constexpr int kMaxAtoms = 128;           // ligand atoms per job on the batched path
 constexpr int kPointAlign = 128;         // pocket conformations padded to this many points
 constexpr int kMaxTemps = GD_MAX_TMP;
-constexpr int kMaxCtaThreads = 512;
+constexpr int kMaxCtaThreads = 512;      // launch bound of the batched kernel (<= 16 replica-warps)
 // c = sqrt(log2(e) / 2): exp(-h^2/2) = 2^-(h c)^2 (scaled hydrogen-bond table entries)
-constexpr double kHdbC = 0.8493218002880191;       // launch bound of the batched kernel (<= 16 replica-warps)
+constexpr double kHdbC = 0.8493218002880191;
 
 // Force-field parameters of one job, in the order the kernels stage them.
 // The FP32 pair code uses algebraically rearranged forms of the reference
