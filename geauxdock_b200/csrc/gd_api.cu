@@ -19,7 +19,7 @@ namespace {
 
 struct Options {
   int kernel = GD_KERNEL_BATCHED;
-  int precision = GD_PREC_FP32;
+  int precision = GD_PREC_FP32_KAHAN;  // FP32 pair terms, compensated reductions
   int warps = 0;  // 0: choose from occupancy
   int kpl = 2;
   int ab = 8;

@@ -1,30 +1,35 @@
 // gd_mc.cu -- the batched Monte Carlo kernel (one warp per replica), the
 // pose-evaluation kernel that shares its energy code, and the replica
-// exchange kernel.
+// exchange kernels.
 //
 // Mapping to the hardware.  The reference runs one 1024-thread block per
 // replica and synchronises the block six or more times per step
 // (src/backend_gpu/kernel_cuda_l1_montecarlo.cu:284-527).  Here one warp owns
 // one replica for a whole chunk of steps: the step needs no block barrier,
 // only warp shuffles.  A CTA holds R replica-warps that share one protein
-// conformation; the CTA stages that conformation, the KDE points and the
-// force-field tables into shared memory with 1-D bulk (TMA) copies once per
-// work item, and the replica-warps then read them for every step.
+// conformation; per work item the CTA stages the force-field tables and the
+// KDE points (and, when it pays, the conformation itself) into shared memory
+// with 1-D bulk (TMA) copies, and its replica-warps read them every step.  A
+// persistent grid takes work items from an atomic queue, heaviest first.
 //
-// Pair loop.  Lane i owns pocket points row+i+32j (j < KPL) in registers and
-// walks the ligand atoms (grouped by atom type) in blocks of AB atoms, so each
-// point is loaded from shared memory once per AB atoms, the per-(atom type,
-// point type) table entries are reloaded only when the atom type changes, and
-// the per-atom hydrophobic sums stay in registers until one warp reduction
-// per atom.  Pocket points are sorted by point type, so neighbouring lanes
-// read the same table entries (shared-memory broadcast).
+// Pair loop, pass 1 (every term but the hydrophobic contact).  Lane i holds
+// pocket points row+i+32j (j < KPL) in registers; the ligand atoms are walked
+// one type group at a time with the (atom type, point type) table entries
+// loaded once per group, and the sparse hydrogen-bond and pocket-specific
+// terms evaluated only for groups where some point of the row needs them.
+// With KPL even, points 2i and 2i+1 of a lane share a register pair and every
+// add, multiply and FMA is one packed f32x2 instruction for both (sm_100);
+// the ligand atom sits in shared memory with every value twice.  Pass 2 (the
+// hydrophobic contact) visits only the rows holding cdc == 1 points and keeps
+// per-atom sums in registers for AB atoms at a time.
 //
-// Arithmetic follows src/backend_gpu/energy_prt_v1.cu:8-174 term by term; the
-// special functions use the single-instruction PTX approximations
-// (rsqrt/rcp/ex2.approx) and powers of 1/d by multiplication.  The
-// FP32-Kahan variant adds each (atom block x point row) partial sum into the
-// lane totals with compensated summation and reduces across lanes with a
-// compensated butterfly; the FP64 variant does the pair arithmetic in double.
+// Arithmetic follows src/backend_gpu/energy_prt_v1.cu:8-174 term by term, in
+// rearranged FP32 forms derived in the comments; the special functions use
+// the single-instruction PTX approximations (rsqrt/rcp/ex2.approx).  The
+// FP32-Kahan variant (the default) adds each row's partial sums of the three
+// dense terms into the lane totals with compensated summation and reduces
+// across lanes with a compensated butterfly; the FP64 variant evaluates the
+// reference's forms in double.
 #include <cstdio>
 #include <type_traits>
 
@@ -323,7 +328,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   // hydrogen-bond and pocket-specific terms are skipped for a group when no
   // lane of the warp has a non-zero parameter for it (both are sparse).
   T s_vdw = 0, s_ele = 0, s_pmf = 0, s_psp = 0, s_hdb = 0;
-  float c_vdw = 0.f, c_ele = 0.f, c_pmf = 0.f, c_psp = 0.f, c_hdb = 0.f;  // Kahan compensations
+  // Kahan compensations of the three dense sums (psp and hdb are short, sparse sums)
+  float c_vdw = 0.f, c_ele = 0.f, c_pmf = 0.f;
   const float *pspc = J.psp + (size_t)iprt * kLigTypes * P;
   const uint32_t *pmc = J.pspmask + (size_t)iprt * P;
   const PairConst kc = PairConst::load(par);
@@ -414,8 +420,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         kahan_add(s_vdw, c_vdw, row_vdw);
         kahan_add(s_ele, c_ele, row_ele);
         kahan_add(s_pmf, c_pmf, row_pmf);
-        kahan_add(s_psp, c_psp, acc.psp);
-        kahan_add(s_hdb, c_hdb, row_hdb);
+        s_psp += acc.psp;
+        s_hdb += row_hdb;
       } else {
         s_vdw += row_vdw;
         s_ele += row_ele;
@@ -493,8 +499,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         kahan_add(s_vdw, c_vdw, acc.vdw);
         kahan_add(s_ele, c_ele, row_ele);
         kahan_add(s_pmf, c_pmf, acc.pmf);
-        kahan_add(s_psp, c_psp, acc.psp);
-        kahan_add(s_hdb, c_hdb, acc.hdb);
+        s_psp += acc.psp;
+        s_hdb += acc.hdb;
       } else {
         s_vdw += acc.vdw;
         s_ele += row_ele;
@@ -590,8 +596,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     vdw = warp_sum_comp(s_vdw, c_vdw);
     ele = warp_sum_comp(s_ele, c_ele);
     pmf = warp_sum_comp(s_pmf, c_pmf);
-    psp = warp_sum_comp(s_psp, c_psp);
-    hdb = warp_sum_comp(s_hdb, c_hdb);
+    psp = warp_sum(s_psp);
+    hdb = warp_sum(s_hdb);
   } else {
     vdw = warp_sum(s_vdw);
     ele = warp_sum(s_ele);

@@ -87,7 +87,8 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
 #define GD_PREC_FP32_KAHAN 1  /* FP32 pair energies, compensated reductions       */
 #define GD_PREC_FP64 2        /* FP64 pair energies                               */
 
-/* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*), "warps" (replicas
+/* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*, default
+ * GD_PREC_FP32_KAHAN), "warps" (replicas
  * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape; default 2, 8),
  * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
  * 0: launch them one by one), "stage" (1: stage each protein conformation in
