@@ -188,7 +188,12 @@ int gdref_load_complex(const char *ligand_id, const char *sdf, const char *ff, c
   // and pocket_center (load.C:285-288) and relies on them starting at zero.
   Ligand0 *lig0 = new Ligand0[MAX_CONF_LIG]();
   Psp0 *psp0 = (Psp0 *)std::calloc(1, sizeof(Psp0));
-  Kde0 *kde0 = (Kde0 *)std::calloc(1, sizeof(Kde0));
+  // loadLHM counts KDE points per type with kde->pns[getLigCode(t)]++
+  // (load.C:1106); an unknown type gives code BADKDE = 50 (data.C:582-584) and pns holds
+  // MAXTP2 = 24 entries (geauxdock.h:252), so the count lands past the struct.
+  // The slack keeps that stray increment inside this allocation; without it the
+  // increment hits whatever the heap put next (here, mcs0[0].x[23]).
+  Kde0 *kde0 = (Kde0 *)std::calloc(1, sizeof(Kde0) + 64 * sizeof(int));
   Mcs0 *mcs0 = (Mcs0 *)std::calloc(MAX_MCS_ROW, sizeof(Mcs0));
   Ligand *ligs = (Ligand *)std::calloc(MAX_CONF_LIG, sizeof(Ligand));
   Psp *psp = (Psp *)std::calloc(1, sizeof(Psp));
