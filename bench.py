@@ -12,7 +12,9 @@ value      pose-evals/s over all ranks, device time (CUDA events on the
 e2e        the same metric through the drop-in C ABI with host buffers
            (SetParaT + CopyH2D + Dock of steps_total = 200, Record copies back)
 roofline   the batched Monte Carlo kernel against the measured FP32 FMA peak
-plain      the plain kernel (the reference's launch structure) on the same work
+plain      the plain kernel (the reference's launch structure) on the same work:
+           all replicas in one launch, and one launch per replica (the plain
+           method's unit of work) on a sample of the replicas
 cpu_baseline  the reference's own CPU Monte Carlo (built from its sources) on
            the box's host cores, a bounded sample of the same workload
 screening  512 ligands of 12-64 atoms (204,800 replicas) in one persistent
@@ -82,6 +84,8 @@ def _args():
     p.add_argument("--screen-intervals", type=int, default=2)
     p.add_argument("--plain-ligands", type=int, default=48,
                    help="ligands of the screening set timed with the plain one-launch-per-ligand kernel")
+    p.add_argument("--plain-replicas", type=int, default=16,
+                   help="replicas of the ensemble timed with the plain kernel, one launch per replica")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     p.add_argument("--serve-steps", type=int, default=2000)
@@ -114,6 +118,15 @@ class Clocks:
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+
+    def wait_first_sample(self, timeout_s: float = 3.0) -> None:
+        """Block until nvidia-smi has written its first sample, so that its
+        start-up (NVML initialisation) is over before the timed region begins."""
+        t0 = time.perf_counter()
+        while self.p is not None and self.p.poll() is None and time.perf_counter() - t0 < timeout_s:
+            if os.path.getsize(self.f.name) > 0:
+                return
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.p is None:
@@ -441,11 +454,14 @@ def run_ours(args) -> None:
     stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     spi = args.mc_steps
-    for _ in range(args.warmup):
-        ens.run(spi, spi)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            ens.run(spi, spi)
+            flush.zero_()
     ens.sync()
     barrier()
     clocks = Clocks(local)
+    clocks.wait_first_sample()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     with torch.cuda.stream(stream):
@@ -497,6 +513,28 @@ def run_ours(args) -> None:
     b.synchronize()
     plain_value = n_rep * STEPS_PER_INTERVAL * p_steps / (a.elapsed_time(b) / 1e3)
     plain.close()
+
+    # ---------------- plain kernel, one replica per launch (the plain method's
+    # unit of work: one complex, one replica), on a strided sample of replicas;
+    # device time of the launches summed, as if issued back to back
+    one_ms, one_launches = 0.0, 0
+    sample = list(range(0, n_rep, max(1, n_rep // args.plain_replicas)))[:args.plain_replicas]
+    for r in sample:
+        h = C.c_void_p()
+        check(lib.gd_ensemble_create_complex_range(C.c_void_p(cx.ctypes.data), r, r, 1000 + rank, local,
+                                                   C.byref(h)))
+        one = dock.Ensemble(h, 1)
+        one.init()
+        one.sync()
+        one.run(STEPS_PER_INTERVAL, 0)
+        ms_r, nl_r = one.sync()
+        one_ms += ms_r
+        one_launches += nl_r
+        one.close()
+    plain_one = {"value": len(sample) * STEPS_PER_INTERVAL / (one_ms / 1e3), "unit": UNIT,
+                 "replicas": len(sample), "launches": one_launches,
+                 "sample": f"{len(sample)} replicas of the ensemble (every {n_rep // len(sample)}th), "
+                           f"{STEPS_PER_INTERVAL} MC steps each, one plain launch per replica, device time"}
     check(lib.gd_set_option(b"kernel", 0))
 
     # ---------------- end to end through the drop-in C ABI, pinned host buffers
@@ -550,7 +588,10 @@ def run_ours(args) -> None:
                          "flops_per_pose_eval": fpp, "avg_launch_ms": avg_launch_ms,
                          "peak_source": "measured this run: FP32 FMA microbenchmark gd_fp32_peak (2 flops/FMA); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain_kernel": {"value": plain_value, "unit": UNIT, "speedup_batched_over_plain": value / world / plain_value},
+            "plain_kernel": {"value": plain_value, "unit": UNIT, "speedup_batched_over_plain": value / world / plain_value,
+                             "launch": "all replicas in one launch (the reference's Dock launch structure)"},
+            "plain_one_replica_per_launch": {**plain_one,
+                                             "speedup_batched_over_plain": value / world / plain_one["value"]},
             "cpu_baseline": cpu,
             "clocks": ck,
             "gpu_launches": all_launches,
