@@ -13,15 +13,18 @@
 // persistent grid takes work items from an atomic queue, heaviest first.
 //
 // Pair loop, pass 1 (every term but the hydrophobic contact).  Lane i holds
-// pocket points row+i+32j (j < KPL) in registers; the ligand atoms are walked
-// one type group at a time with the (atom type, point type) table entries
-// loaded once per group, and the sparse hydrogen-bond and pocket-specific
-// terms evaluated only for groups where some point of the row needs them.
-// With KPL even, points 2i and 2i+1 of a lane share a register pair and every
-// add, multiply and FMA is one packed f32x2 instruction for both (sm_100);
-// the ligand atom sits in shared memory with every value twice.  Pass 2 (the
-// hydrophobic contact) visits only the rows holding cdc == 1 points and keeps
-// per-atom sums in registers for AB atoms at a time.
+// pocket points row+i+32j (j < KPL) in registers.  The FP32 ligand sits in
+// shared memory as atom pairs, and with KPL even every add, multiply and FMA
+// evaluates atoms 2k and 2k+1 against one point as one packed f32x2
+// instruction (sm_100).  Per work item the CTA builds from the per-type tables
+// one entry per (atom pair, point type) with the two atoms' values interleaved,
+// so the loop walks atom pairs with no grouping by atom type; the sparse
+// hydrogen-bond and pocket-specific terms are evaluated only for the atom pairs
+// where some point of the row needs them.  With KPL = 1 (and in FP64) the atoms
+// are walked one type group at a time in scalar arithmetic instead.  Pass 2
+// (the hydrophobic contact) visits only the rows holding cdc == 1 points, packed
+// over atom pairs the same way, and keeps per-atom sums in registers for AB
+// atoms at a time.
 //
 // Arithmetic follows src/backend_gpu/energy_prt_v1.cu:8-174 term by term, in
 // rearranged FP32 forms derived in the comments; the special functions use
@@ -57,13 +60,18 @@ struct alignas(16) V4 {
   T x, y, z, w;
 };
 
-// FP32 ligand atom in shared memory with every value twice, so that packed
-// f32x2 arithmetic against two pocket points reads it as one register pair.
-struct alignas(16) LigAtom2 {
+// FP32 ligand in shared memory as atom pairs: component k of each float2 is
+// atom 2i + k of pair i, so that packed f32x2 arithmetic reads two atoms as one
+// register pair.  An odd atom count ends with an inert dummy half.
+struct alignas(16) LigPair {
   float2 x, y, z, q;
 };
-__device__ __forceinline__ V4<float> unpack(const LigAtom2 &a) { return V4<float>{a.x.x, a.y.x, a.z.x, a.q.x}; }
-__device__ __forceinline__ V4<double> unpack(const V4<double> &a) { return a; }
+__device__ __forceinline__ V4<float> atom_at(const LigPair *lig, int a)
+{
+  const float *f = reinterpret_cast<const float *>(lig + (a >> 1)) + (a & 1);
+  return V4<float>{f[0], f[2], f[4], f[6]};
+}
+__device__ __forceinline__ V4<double> atom_at(const V4<double> *lig, int a) { return lig[a]; }
 
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 
@@ -73,7 +81,7 @@ __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 // ----------------------------------------------------------- smem layout --
 struct SmemLayout {
-  uint32_t params, lgrp, pos, aux, kde, warp0, warp_bytes, lig_bytes, total;
+  uint32_t params, lgrp, pos, aux, kde, apt, aph, ahd, warp0, warp_bytes, lig_bytes, total;
 };
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
@@ -92,8 +100,15 @@ __host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots,
   off = align16(off + 8u * (uint32_t)P);
   s.kde = off;
   off = align16(off + 16u * (uint32_t)Kst);
-  s.lig_bytes = (uint32_t)lig_slots * 32u;  // LigAtom2 (FP32) or V4<double> (FP64)
-  (void)fp64;
+  // FP32: per (atom pair, point type) tables of the atom-pair pair loop
+  const uint32_t npairs = fp64 ? 0u : (uint32_t)(lig_slots + 1) / 2u;
+  s.apt = off;
+  off = align16(off + 32u * (uint32_t)kTabCols * npairs);
+  s.aph = off;
+  off = align16(off + 16u * (uint32_t)kTabCols * npairs);
+  s.ahd = off;
+  off = align16(off + 16u * npairs);
+  s.lig_bytes = (uint32_t)lig_slots * (fp64 ? 32u : 16u);  // V4<double> per atom, or LigPair per two atoms
   // per warp: rotated ligand, ReplicaMC state, EnergyScratch (192 B), WarpStats (64 B)
   s.warp_bytes = align16(s.lig_bytes + (uint32_t)sizeof(ReplicaMC) + 192u + 64u);
   s.warp0 = off;
@@ -155,7 +170,7 @@ __device__ __forceinline__ void pair_atoms(const LA *lig, int a, int aend, const
   if constexpr (PREC == kFP64) {
     const double lj0 = c.lj0, lj1 = c.lj1, el0 = c.el0, el1 = c.el1, a1 = c.a1, b1 = c.b1;
     for (; a < aend; ++a) {
-      const V4<double> la = unpack(lig[a]);
+      const V4<double> la = atom_at(lig, a);
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         const double dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -181,7 +196,7 @@ __device__ __forceinline__ void pair_atoms(const LA *lig, int a, int aend, const
   } else {
 #pragma unroll 2
     for (; a < aend; ++a) {
-      const V4<float> la = unpack(lig[a]);
+      const V4<float> la = atom_at(lig, a);
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         const float dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -208,64 +223,100 @@ __device__ __forceinline__ void pair_atoms(const LA *lig, int a, int aend, const
   }
 }
 
-// Running sums of one point row in the packed form: component k of each
-// float2 belongs to point 2i + k of the lane's pair i.
-template <int KP>
-struct PairAcc2 {
-  float2 vdw[KP], pmf[KP], hdb[KP], ele[KP];
+// Running sums of one point row in the atom-pair form: component k of each
+// float2 belongs to atom 2i + k of the pair being visited; the electrostatic
+// sums are kept per point (they are multiplied by the point charge at the end
+// of the row).
+template <int KPL>
+struct PairAccP {
+  float2 vdw, pmf, hdb;
+  float2 ele[KPL];
   float psp;
 };
 
-// Per type group, per point pair: the table entries as register pairs.
-template <int KP>
-struct PairTab2 {
-  float2 inva[KP], nba[KP], npmf0[KP], pmf1[KP], h1c[KP], h0c[KP];
-};
+// Per work item, shared-memory tables of the atom-pair pair loop, built from
+// the per-type tables: for pair i (atoms a = 2i, b = 2i + 1) and point type pt,
+// e = i * kTabCols + pt,
+//   apt[2e]     = (1/p1a, -p2a/p1a) of a and b interleaved: (a.x, b.x, a.y, b.y)
+//   apt[2e + 1] = (-pmf0, pmf1) interleaved
+//   aph[e]      = (hdb1 c, -hdb0 hdb1 c) interleaved
+//   ahd[i]      = (point types with hydrogen-bond parameters for a or b,
+//                  bit set of the types of a and b, type of a, type of b or 31).
+// The dummy half of an odd atom count gets the padding column and no types:
+// every term of it is exactly 0.
+__device__ void build_pair_tables(int L, const DevParams *par, const int2 *lg, float4 *apt, float4 *aph, int4 *ahd)
+{
+  const int npairs = (L + 1) >> 1;
+  for (int e = threadIdx.x; e < npairs * kTabCols; e += blockDim.x) {
+    const int i = e / kTabCols, pt = e % kTabCols;
+    const int a = 2 * i, b = a + 1;
+    const int lta = lg[a].x, ltb = b < L ? lg[b].x : -1;
+    const float4 ta = par->tab4[lta][pt];
+    const float4 tb = ltb >= 0 ? par->tab4[ltb][pt] : tab4_padding();
+    apt[2 * e] = make_float4(ta.x, tb.x, ta.y, tb.y);
+    apt[2 * e + 1] = make_float4(ta.z, tb.z, ta.w, tb.w);
+    const float2 ha = par->tab2[lta][pt], hb = ltb >= 0 ? par->tab2[ltb][pt] : make_float2(0.f, 0.f);
+    aph[e] = make_float4(ha.x, hb.x, ha.y, hb.y);
+    if (pt == 0) {
+      const uint32_t hm = par->hdbmask[lta] | (ltb >= 0 ? par->hdbmask[ltb] : 0u);
+      const uint32_t tb_bits = (1u << lta) | (ltb >= 0 ? 1u << ltb : 0u);
+      ahd[i] = make_int4((int)hm, (int)tb_bits, lta, ltb >= 0 ? ltb : 31);
+    }
+  }
+}
 
-// Packed (f32x2) twin of the FP32 branch of pair_atoms: the same operations
-// in the same order, two pocket points per instruction (__ffma2_rn /
+// Pair terms of ligand atom pair i against the lane's KPL points
+// (energy_prt_v1.cu:56-139 except the hydrophobic contact), the FP32 forms of
+// pair_atoms with two atoms per packed f32x2 instruction (__ffma2_rn /
 // __fadd2_rn / __fmul2_rn, sm_100); the special functions stay per component.
-// npx/npy/npz hold the negated point coordinates (x_atom - x_point is
-// x_atom + (-x_point), exactly).
-template <int KP, bool HDB, bool PSP>
-__device__ __forceinline__ void pair_atoms_x2(const LigAtom2 *lig, int a, int aend, const float2 (&npx)[KP],
-                                              const float2 (&npy)[KP], const float2 (&npz)[KP],
-                                              const PairTab2<KP> &t, const float (&tps)[2 * KP],
-                                              const PairConst &c, PairAcc2<KP> &acc)
+// HDB / PSP: evaluate the hydrogen-bond / pocket-specific terms (some point of
+// the row has a parameter for one of the two atoms).  npx/npy/npz hold the
+// lane's negated point coordinates twice (x_atom - x_point is x_atom + (-x_point),
+// exactly); the charges and, for PSP, the two atom types are read from shared
+// memory where they are used, which keeps the loop within its registers.
+template <int KPL, bool HDB, bool PSP>
+__device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i, const float2 &lx,
+                                               const float2 &ly, const float2 &lz, const float4 *__restrict__ apt,
+                                               const float4 *__restrict__ aph, const int4 *__restrict__ ahd,
+                                               const int (&pt)[KPL], const uint32_t (&pm)[KPL],
+                                               const float2 (&npx)[KPL], const float2 (&npy)[KPL],
+                                               const float2 (&npz)[KPL], const float *__restrict__ pspc, int P,
+                                               int row, int lane, const PairConst &c, PairAccP<KPL> &acc)
 {
   const float2 lj01 = f2(c.lj01), lj0 = f2(c.lj0), one = f2(1.0f), inv_el1 = f2(c.inv_el1);
   const float2 za = f2(-0.5f * kLog2e), zb = f2(6.0f * kLog2e);
-#pragma unroll 2
-  for (; a < aend; ++a) {
-    const LigAtom2 la = lig[a];
 #pragma unroll
-    for (int i = 0; i < KP; ++i) {
-      const float2 dx = __fadd2_rn(la.x, npx[i]), dy = __fadd2_rn(la.y, npy[i]), dz = __fadd2_rn(la.z, npz[i]);
-      const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-      const float2 r = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
-      const float2 d = __fmul2_rn(d2, r);
-      const float2 d3 = __fmul2_rn(d2, d);
-      const float2 d6 = __fmul2_rn(d3, d3);
-      const float2 den = __ffma2_rn(__fmul2_rn(d6, d3), t.inva[i], __ffma2_rn(lj01, d2, lj0));
-      const float2 num = __ffma2_rn(t.nba[i], d3, one);
-      acc.vdw[i] = __ffma2_rn(num, make_float2(rcp_approx(den.x), rcp_approx(den.y)), acc.vdw[i]);
-      float2 g = __fmul2_rn(r, inv_el1);
-      if (d2.x < c.ed2) g.x = fmaf(d2.x, fmaf(c.eb, d.x, c.ea), c.el0);
-      if (d2.y < c.ed2) g.y = fmaf(d2.y, fmaf(c.eb, d.y, c.ea), c.el0);
-      acc.ele[i] = __ffma2_rn(la.q, g, acc.ele[i]);
-      const float2 dmp = __fadd2_rn(d, t.npmf0[i]);
-      const float2 z = __fmul2_rn(__ffma2_rn(za, d, zb), dmp);
-      const float2 e1 = __fadd2_rn(make_float2(ex2_approx(z.x), ex2_approx(z.y)), one);
-      acc.pmf[i] = __ffma2_rn(t.pmf1[i], make_float2(rcp_approx(e1.x), rcp_approx(e1.y)), acc.pmf[i]);
-      if constexpr (PSP) {
-        acc.psp += (dmp.x <= 0.0f) ? tps[2 * i] : 0.0f;
-        acc.psp += (dmp.y <= 0.0f) ? tps[2 * i + 1] : 0.0f;
-      }
-      if constexpr (HDB) {
-        const float2 h = __ffma2_rn(d, t.h1c[i], t.h0c[i]);
-        const float2 hh = __fmul2_rn(h, h);
-        acc.hdb[i] = __ffma2_rn(t.h1c[i], make_float2(ex2_approx(-hh.x), ex2_approx(-hh.y)), acc.hdb[i]);
-      }
+  for (int j = 0; j < KPL; ++j) {
+    const int e = i * kTabCols + pt[j];
+    const float4 ta = apt[2 * e], tb = apt[2 * e + 1];
+    const float2 dx = __fadd2_rn(lx, npx[j]), dy = __fadd2_rn(ly, npy[j]), dz = __fadd2_rn(lz, npz[j]);
+    const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    const float2 r = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
+    const float2 d = __fmul2_rn(d2, r);
+    const float2 d3 = __fmul2_rn(d2, d);
+    const float2 d6 = __fmul2_rn(d3, d3);
+    const float2 den = __ffma2_rn(__fmul2_rn(d6, d3), make_float2(ta.x, ta.y), __ffma2_rn(lj01, d2, lj0));
+    const float2 num = __ffma2_rn(make_float2(ta.z, ta.w), d3, one);
+    acc.vdw = __ffma2_rn(num, make_float2(rcp_approx(den.x), rcp_approx(den.y)), acc.vdw);
+    float2 g = __fmul2_rn(r, inv_el1);
+    if (d2.x < c.ed2) g.x = fmaf(d2.x, fmaf(c.eb, d.x, c.ea), c.el0);
+    if (d2.y < c.ed2) g.y = fmaf(d2.y, fmaf(c.eb, d.y, c.ea), c.el0);
+    acc.ele[j] = __ffma2_rn(lig[i].q, g, acc.ele[j]);
+    const float2 dmp = __fadd2_rn(d, make_float2(tb.x, tb.y));
+    const float2 z = __fmul2_rn(__ffma2_rn(za, d, zb), dmp);
+    const float2 e1 = __fadd2_rn(make_float2(ex2_approx(z.x), ex2_approx(z.y)), one);
+    acc.pmf = __ffma2_rn(make_float2(tb.z, tb.w), make_float2(rcp_approx(e1.x), rcp_approx(e1.y)), acc.pmf);
+    if constexpr (PSP) {
+      const int p = row + 32 * j + lane;
+      const int lta = ahd[i].z, ltb = ahd[i].w;
+      if (((pm[j] >> lta) & 1u) && dmp.x <= 0.0f) acc.psp += __ldg(pspc + (size_t)lta * P + p);
+      if (((pm[j] >> ltb) & 1u) && dmp.y <= 0.0f) acc.psp += __ldg(pspc + (size_t)ltb * P + p);
+    }
+    if constexpr (HDB) {
+      const float4 th = aph[e];
+      const float2 h = __ffma2_rn(d, make_float2(th.x, th.y), make_float2(th.z, th.w));
+      const float2 hh = __fmul2_rn(h, h);
+      acc.hdb = __ffma2_rn(make_float2(th.x, th.y), make_float2(ex2_approx(-hh.x), ex2_approx(-hh.y)), acc.hdb);
     }
   }
 }
@@ -274,13 +325,15 @@ template <int PREC, int KPL, int AB>
 __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__restrict__ par,
                                          const float4 *__restrict__ pos, const float2 *__restrict__ aux,
                                          const float4 *__restrict__ kde, const int2 *__restrict__ lgrp,
-                                         void *ligbuf, int ilig, int iprt, const float *mm, EnergyScratch *out)
+                                         const float4 *__restrict__ apt, const float4 *__restrict__ aph,
+                                         const int4 *__restrict__ ahd, void *ligbuf, int ilig, int iprt,
+                                         const float *mm, EnergyScratch *out)
 {
   using T = typename std::conditional<PREC == kFP64, double, float>::type;
   const int lane = lane_id();
   const int L = J.natom;
   const int P = J.npoint_pad;
-  using LA = typename std::conditional<PREC == kFP64, V4<double>, LigAtom2>::type;
+  using LA = typename std::conditional<PREC == kFP64, V4<double>, LigPair>::type;
   LA *lig = reinterpret_cast<LA *>(ligbuf);
 
   // rotation + translation, kernel_cuda_l1_montecarlo.cu:336-380
@@ -316,8 +369,26 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     o.y = r10 * (T)v.x + r11 * (T)v.y + r12 * (T)v.z + ty;
     o.z = r20 * (T)v.x + r21 * (T)v.y + r22 * (T)v.z + tz;
     o.w = (T)v.w;
-    if constexpr (PREC == kFP64) lig[a] = o;
-    else lig[a] = LigAtom2{f2(o.x), f2(o.y), f2(o.z), f2(o.w)};
+    if constexpr (PREC == kFP64) {
+      lig[a] = o;
+    } else {
+      float *f = reinterpret_cast<float *>(lig + (a >> 1)) + (a & 1);
+      f[0] = o.x;
+      f[2] = o.y;
+      f[4] = o.z;
+      f[6] = o.w;
+    }
+  }
+  if constexpr (PREC != kFP64) {
+    // the dummy half of an odd atom count: far from every point (padding
+    // points sit near +1e4), no charge; its table entries make every term 0
+    if ((L & 1) && lane == 0) {
+      float *f = reinterpret_cast<float *>(lig + (L >> 1)) + 1;
+      f[0] = -1.0e4f;
+      f[2] = -1.0e4f;
+      f[4] = -1.0e4f;
+      f[6] = 0.0f;
+    }
   }
   __syncwarp();
 
@@ -335,10 +406,12 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   const PairConst kc = PairConst::load(par);
 
   if constexpr (PREC != kFP64 && KPL % 2 == 0) {
-    // packed form: the lane's points 2i and 2i+1 share one register pair
-    constexpr int KP = KPL / 2;
+    // atom-pair form: atoms 2i and 2i+1 share one register pair and the
+    // table entries come per atom pair, so there is no loop over type groups
+    const LigPair *lp = lig;
+    const int npairs = (L + 1) >> 1;
     for (int row = 0; row < P; row += 32 * KPL) {
-      float2 npx[KP], npy[KP], npz[KP];
+      float2 npx[KPL], npy[KPL], npz[KPL];
       int pt[KPL];
       uint32_t pm[KPL];
       uint32_t ptbits = 0u, pmbits = 0u;
@@ -346,76 +419,50 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       for (int j = 0; j < KPL; ++j) {
         const int p = row + 32 * j + lane;
         const float4 q = pos[p];
-        if (j & 1) {
-          npx[j / 2].y = -q.x; npy[j / 2].y = -q.y; npz[j / 2].y = -q.z;
-        } else {
-          npx[j / 2].x = -q.x; npy[j / 2].x = -q.y; npz[j / 2].x = -q.z;
-        }
+        npx[j] = f2(-q.x);
+        npy[j] = f2(-q.y);
+        npz[j] = f2(-q.z);
         pt[j] = __float_as_int(aux[p].y);
         pm[j] = __ldg(pmc + p);
         ptbits |= 1u << pt[j];
         pmbits |= pm[j];
       }
+      // point types present in the row, and ligand types with a pocket-specific
+      // potential on some point of it: decide per atom pair, for the whole warp,
+      // whether the sparse terms are evaluated
       ptbits = __reduce_or_sync(0xffffffffu, ptbits);
       pmbits = __reduce_or_sync(0xffffffffu, pmbits);
-      PairAcc2<KP> acc;
+      PairAccP<KPL> acc;
+      acc.vdw = acc.pmf = acc.hdb = f2(0.0f);
 #pragma unroll
-      for (int i = 0; i < KP; ++i) acc.vdw[i] = acc.pmf[i] = acc.hdb[i] = acc.ele[i] = f2(0.0f);
+      for (int j = 0; j < KPL; ++j) acc.ele[j] = f2(0.0f);
       acc.psp = 0.0f;
-      int a = 0;
-      while (a < L) {
-        const int2 grp = lgrp[a];
-        const int lt = grp.x, aend = grp.y;
-        const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
-        const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
-        PairTab2<KP> tb;
-        float tps[KPL];
-#pragma unroll
-        for (int j = 0; j < KPL; ++j) {
-          const float4 t4 = par->tab4[lt][pt[j]];
-          if (j & 1) {
-            tb.inva[j / 2].y = t4.x; tb.nba[j / 2].y = t4.y; tb.npmf0[j / 2].y = t4.z; tb.pmf1[j / 2].y = t4.w;
-          } else {
-            tb.inva[j / 2].x = t4.x; tb.nba[j / 2].x = t4.y; tb.npmf0[j / 2].x = t4.z; tb.pmf1[j / 2].x = t4.w;
-          }
-          tps[j] = 0.0f;
-        }
-#pragma unroll
-        for (int i = 0; i < KP; ++i) tb.h1c[i] = tb.h0c[i] = f2(0.0f);
+      for (int i = 0; i < npairs; ++i) {
+        const int2 fl = *reinterpret_cast<const int2 *>(&ahd[i].x);
+        const bool any_hdb = ((uint32_t)fl.x & ptbits) != 0u;
+        const bool any_psp = ((uint32_t)fl.y & pmbits) != 0u;
+        const float4 l01 = *reinterpret_cast<const float4 *>(&lp[i].x);
+        const float2 lx = make_float2(l01.x, l01.y), ly = make_float2(l01.z, l01.w), lz = lp[i].z;
         if (any_hdb) {
-#pragma unroll
-          for (int j = 0; j < KPL; ++j) {
-            const float2 t2 = par->tab2[lt][pt[j]];
-            if (j & 1) {
-              tb.h1c[j / 2].y = t2.x; tb.h0c[j / 2].y = t2.y;
-            } else {
-              tb.h1c[j / 2].x = t2.x; tb.h0c[j / 2].x = t2.y;
-            }
-          }
-        }
-        if (any_psp) {
-#pragma unroll
-          for (int j = 0; j < KPL; ++j)
-            if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
-        }
-        if (any_hdb) {
-          if (any_psp) pair_atoms_x2<KP, true, true>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
-          else pair_atoms_x2<KP, true, false>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+          if (any_psp)
+            pair_atom_pair<KPL, true, true>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+          else
+            pair_atom_pair<KPL, true, false>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         } else {
-          if (any_psp) pair_atoms_x2<KP, false, true>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
-          else pair_atoms_x2<KP, false, false>(lig, a, aend, npx, npy, npz, tb, tps, kc, acc);
+          if (any_psp)
+            pair_atom_pair<KPL, false, true>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+          else
+            pair_atom_pair<KPL, false, false>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         }
-        a = aend;
       }
-      float row_vdw = 0.f, row_ele = 0.f, row_pmf = 0.f, row_hdb = 0.f;
+      float row_ele = 0.f;
 #pragma unroll
-      for (int i = 0; i < KP; ++i) {
-        row_vdw += acc.vdw[i].x + acc.vdw[i].y;
-        row_pmf += acc.pmf[i].x + acc.pmf[i].y;
-        row_hdb += acc.hdb[i].x + acc.hdb[i].y;
+      for (int j = 0; j < KPL; ++j) {
         // the point charges are read again here rather than held through the atom loop
-        row_ele += pos[row + 64 * i + lane].w * acc.ele[i].x + pos[row + 64 * i + 32 + lane].w * acc.ele[i].y;
+        row_ele += pos[row + 32 * j + lane].w * (acc.ele[j].x + acc.ele[j].y);
       }
+      const float row_vdw = acc.vdw.x + acc.vdw.y, row_pmf = acc.pmf.x + acc.pmf.y;
+      const float row_hdb = acc.hdb.x + acc.hdb.y;
       if constexpr (PREC == kFP32Kahan) {
         kahan_add(s_vdw, c_vdw, row_vdw);
         kahan_add(s_ele, c_ele, row_ele);
@@ -534,27 +581,36 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           ph[j] = aux[p].x;
         }
         if constexpr (PREC != kFP64 && KPL % 2 == 0) {
-          // packed form, the same operations per component
+          // atom-pair form, the same operations per component: hpc[2k] and
+          // hpc[2k+1] are atoms a0 + 2k and a0 + 2k + 1 (AB is even)
           const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f), c2 = f2(-0.5f / 81.0f);
+          float2 npx[KPL], npy[KPL], npz[KPL], ph2[KPL];
 #pragma unroll
-          for (int k = 0; k < AB; ++k) {
-            const int a = a0 + k;
+          for (int j = 0; j < KPL; ++j) {
+            npx[j] = f2(-px[j]);
+            npy[j] = f2(-py[j]);
+            npz[j] = f2(-pz[j]);
+            ph2[j] = f2(ph[j]);
+          }
+#pragma unroll
+          for (int k = 0; k < AB / 2; ++k) {
+            const int a = a0 + 2 * k;
             if (a >= L) break;
-            const LigAtom2 la = lig[a];
+            const LigPair la = lig[a >> 1];
+            float2 h2 = make_float2(hpc[2 * k], hpc[2 * k + 1]);
 #pragma unroll
-            for (int i = 0; i < KPL / 2; ++i) {
-              const float2 dx = __fadd2_rn(la.x, make_float2(-px[2 * i], -px[2 * i + 1]));
-              const float2 dy = __fadd2_rn(la.y, make_float2(-py[2 * i], -py[2 * i + 1]));
-              const float2 dz = __fadd2_rn(la.z, make_float2(-pz[2 * i], -pz[2 * i + 1]));
+            for (int j = 0; j < KPL; ++j) {
+              const float2 dx = __fadd2_rn(la.x, npx[j]), dy = __fadd2_rn(la.y, npy[j]), dz = __fadd2_rn(la.z, npz[j]);
               const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
               float2 t = __ffma2_rn(d2, c1, one);
               t.x = fmaxf(t.x, 0.0f);
               t.y = fmaxf(t.y, 0.0f);
               const float2 u = __ffma2_rn(d2, c2, one);
               const float2 w = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, t), t), u);
-              hpc[k] = fmaf(ph[2 * i], w.x, hpc[k]);
-              hpc[k] = fmaf(ph[2 * i + 1], w.y, hpc[k]);
+              h2 = __ffma2_rn(ph2[j], w, h2);
             }
+            hpc[2 * k] = h2.x;
+            hpc[2 * k + 1] = h2.y;
           }
           continue;
         }
@@ -562,7 +618,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         for (int k = 0; k < AB; ++k) {
           const int a = a0 + k;
           if (a >= L) break;
-          const V4<T> la = unpack(lig[a]);
+          const V4<T> la = atom_at(lig, a);
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
             const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
@@ -618,7 +674,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       const int cnt = J.kcnt[lt];
       if (cnt == 0) continue;
       const int beg = J.kbeg[lt];
-      const V4<T> la = unpack(lig[a]);
+      const V4<T> la = atom_at(lig, a);
       const T inv = (T)1 / (T)cnt;
       for (int k = beg + lane; k < beg + cnt; k += 32) {
         const float4 q = kde[k];
@@ -645,7 +701,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         for (int a = 0; a < L; ++a) {
           const float4 q = J.mcs[(size_t)a * M + m];
           if (q.w != 0.0f) {
-            const V4<T> la = unpack(lig[a]);
+            const V4<T> la = atom_at(lig, a);
             const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
             s += dx * dx + dy * dy + dz * dz;
             ++n;
@@ -763,10 +819,20 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         mbar_wait(&bar, phase ^ 1u, A.wait_limit ? A.wait_limit : kWaitLimit);
         return;
       }
+      if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+        __syncthreads();  // parameters and type groups are in shared memory
+        if (wi.job != prev_job)
+          build_pair_tables(J.natom, reinterpret_cast<const DevParams *>(smem + sl.params),
+                            reinterpret_cast<const int2 *>(smem + sl.lgrp), reinterpret_cast<float4 *>(smem + sl.apt),
+                            reinterpret_cast<float4 *>(smem + sl.aph), reinterpret_cast<int4 *>(smem + sl.ahd));
+      }
       prev_job = wi.job;
       prev_prt = wi.prt;
     }
     __syncthreads();
+    const float4 *apt = reinterpret_cast<const float4 *>(smem + sl.apt);
+    const float4 *aph = reinterpret_cast<const float4 *>(smem + sl.aph);
+    const int4 *ahd = reinterpret_cast<const int4 *>(smem + sl.ahd);
 
     const DevParams *par = reinterpret_cast<const DevParams *>(smem + sl.params);
     // the protein conformation: staged in shared memory, or read through L1
@@ -789,7 +855,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         const int ilig = A.conf[2 * r], iprt = A.conf[2 * r + 1];
         if (lane < 6) esc->mm[lane] = A.mm[6 * r + lane];
         __syncwarp();
-        energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, ligbuf, ilig, iprt, esc->mm, esc);
+        energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, apt, aph, ahd, ligbuf, ilig, iprt, esc->mm, esc);
         if (lane < 10) {
           A.out[10 * (size_t)r + lane] = (float)esc->e[lane];
           if (A.out64) A.out64[10 * (size_t)r + lane] = esc->e[lane];
@@ -854,7 +920,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
             esc->mm[lane] = __fmaf_rn(par->move_scale[lane], 0.0f, srep->movematrix[lane]);
           }
           __syncwarp();
-          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, ligbuf, ilig, iprt, esc->mm, esc);
+          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, apt, aph, ahd, ligbuf, ilig, iprt, esc->mm, esc);
           const float etot = (float)esc->e[9];
 
           // Metropolis test in FP64, kernel_cuda_l1_montecarlo.cu:485-507
@@ -1009,8 +1075,9 @@ __global__ void __launch_bounds__(256) eval_global_kernel(const DevJob *jobp, co
     if (lane < 6) esc->mm[lane] = mm[6 * (size_t)i + lane];
     __syncwarp();
     const size_t P = (size_t)J.npoint_pad;
-    energy_warp<PREC, KPL, AB>(J, J.par, J.pos + iprt * P, J.aux + iprt * P, J.kde, J.lgrp, wb, ilig, iprt, esc->mm,
-                               esc);
+    // KPL = 1: the per-type-group form, which needs no per-work-item tables
+    energy_warp<PREC, KPL, AB>(J, J.par, J.pos + iprt * P, J.aux + iprt * P, J.kde, J.lgrp, nullptr, nullptr, nullptr,
+                               wb, ilig, iprt, esc->mm, esc);
     if (lane < 10) out[10 * (size_t)i + lane] = (float)esc->e[lane];
     if (raw && lane < 9) raw[9 * (size_t)i + lane] = (float)esc->raw[lane];
     __syncwarp();
