@@ -48,12 +48,12 @@ METRIC = "MC pose-evals/s batched+served vs plain kernel on 1 B200; p50/p99 dock
 UNIT = "pose-evals/s"
 STEPS_PER_INTERVAL = 50
 # DRAM bytes (read + write) of one Monte Carlo launch of this workload (3520
-# replicas x 50 steps, tile 8 x kpl 2 x ab 8), measured with
+# replicas x 50 steps, tile 8 x kpl 2 x ab 8, pocket read through L1), measured with
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:mc_kernel -s 4 -c 1
-#       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,2,8
-# (2,075,648 B read + 7,424 B written); it does not grow with the steps per launch.
-TRAFFIC_BYTES_PER_LAUNCH = 2_075_648 + 7_424
+#       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,2,8,0
+# (1,816,064 B read + 99,328 B written); it does not grow with the steps per launch.
+TRAFFIC_BYTES_PER_LAUNCH = 1_816_064 + 99_328
 
 
 def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
