@@ -666,23 +666,32 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
 
   // ---- KDE, energy_kde_v1.cu:183-274: per atom, mean of exp(kde2 d^2) over
   // the KDE points of the same type; atoms with no such point contribute 0.
+  // One type group at a time: lane k holds KDE point k of the group's type and
+  // sums over the group's atoms, then scales by 1 / (points of the type).
   T kacc = 0;
   {
     const T kde2 = par->kde2;
-    for (int a = 0; a < L; ++a) {
-      const int lt = lgrp[a].x;
+    for (int a = 0; a < L;) {
+      const int2 grp = lgrp[a];
+      const int lt = grp.x, aend = grp.y;
       const int cnt = J.kcnt[lt];
-      if (cnt == 0) continue;
-      const int beg = J.kbeg[lt];
-      const V4<T> la = atom_at(lig, a);
-      const T inv = (T)1 / (T)cnt;
-      for (int k = beg + lane; k < beg + cnt; k += 32) {
-        const float4 q = kde[k];
-        const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
-        const T d2 = dx * dx + dy * dy + dz * dz;
-        if constexpr (PREC == kFP64) kacc += exp(kde2 * d2) * inv;
-        else kacc += ex2_approx((kde2 * kLog2e) * d2) * inv;
+      if (cnt > 0) {
+        const int beg = J.kbeg[lt];
+        const T inv = (T)1 / (T)cnt;
+        for (int k = beg + lane; k < beg + cnt; k += 32) {
+          const float4 q = kde[k];
+          T s = 0;
+          for (int b = a; b < aend; ++b) {
+            const V4<T> la = atom_at(lig, b);
+            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+            const T d2 = dx * dx + dy * dy + dz * dz;
+            if constexpr (PREC == kFP64) s += exp(kde2 * d2);
+            else s += ex2_approx((kde2 * kLog2e) * d2);
+          }
+          kacc += s * inv;
+        }
       }
+      a = aend;
     }
   }
   T ekde;

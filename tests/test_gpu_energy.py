@@ -89,6 +89,23 @@ def test_edge_sizes(lib, enepara, oracle_lib):
         _check(out, _oracle_energies(oracle_lib, cx, conf, mm), TOL32, f"L={L} P={P}")
 
 
+@pytest.mark.parametrize("L", [127, 128])
+def test_batched_atom_cap(lib, enepara, oracle_lib, L):
+    """The batched path's atom cap (128, beyond the Complex's 64): the largest
+    per-atom-pair tables, and an odd count whose last pair has a dummy half."""
+    rng = np.random.default_rng(L)
+    pk = synth.make_pocket(rng, 700, 2)
+    job = synth.make_job(rng, pk, L, 2, 300, 6, [1.0], seed=L)
+    n = 24
+    mm = synth.config4_poses(L, n, radius=4.0)
+    conf = np.stack([np.arange(n) % 2, (np.arange(n) // 2) % 2], axis=1).astype(np.int32)
+    e_or, _ = oracle_lib.energy_desc(pk, job, enepara, conf, mm)
+    with dock.Ensemble.from_jobs([pk], [job], enepara) as e:
+        for prec in (GD_PREC_FP32, GD_PREC_FP32_KAHAN):
+            out, _, _ = e.eval_poses(0, conf, mm, prec)
+            _check(out, e_or, TOL32, f"L={L} precision {prec}")
+
+
 def test_reference_fp32_direct(lib, enepara, oracle_lib):
     """GPU against the reference's own CPU energy routine run here (oracle/_ref),
     on config 2 (40 atoms x 1500 points): the GPU is within 1e-5 of FP64, and
