@@ -11,7 +11,8 @@ value      pose-evals/s over all ranks, device time (CUDA events on the
            library's stream), inputs resident in HBM, L2 flushed between steps
 e2e        the same metric through the drop-in C ABI with host buffers
            (SetParaT + CopyH2D + Dock of steps_total = 200, Record copies back)
-roofline   the batched Monte Carlo kernel against the measured FP32 FMA peak
+roofline   the batched Monte Carlo kernel against the measured FP32 FMA peak, and
+           its special-function (MUFU) pipe use against the nominal MUFU rate
 plain      the plain kernel (the reference's launch structure) on the same work:
            all replicas in one launch, and one launch per replica (the plain
            method's unit of work) on a sample of the replicas
@@ -52,8 +53,8 @@ STEPS_PER_INTERVAL = 50
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:mc_kernel -s 4 -c 1
 #       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,2,8,0
-# (1,816,064 B read + 99,328 B written); it does not grow with the steps per launch.
-TRAFFIC_BYTES_PER_LAUNCH = 1_816_064 + 99_328
+# (1,811,968 B read + 52,224 B written); it does not grow with the steps per launch.
+TRAFFIC_BYTES_PER_LAUNCH = 1_811_968 + 52_224
 
 
 def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
@@ -246,6 +247,22 @@ def _hbm_share(launch_ms: float) -> dict:
     gbs = TRAFFIC_BYTES_PER_LAUNCH / (launch_ms / 1e3) / 1e9
     return {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak if peak else None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peak else "unavailable"}
+
+
+def _mufu_share(natom: int, npoint: int, pose_evals_per_s: float, sm_mhz) -> dict:
+    """Special-function (MUFU) pipe use of the Monte Carlo launch: the pair loop's
+    4 MUFU ops per ligand atom x padded pocket point (rsqrt, rcp for Lennard-Jones,
+    ex2 and rcp for the pmf sigmoid) against 16 per clock per SM x 148 SMs at the
+    SM clock sampled during the timed region."""
+    ppad = -(-npoint // 128) * 128
+    ops = 4 * natom * ppad
+    if not sm_mhz:
+        return {"ops_per_pose_eval": ops, "frac": None}
+    achieved = ops * pose_evals_per_s / 1e9
+    peak = 16 * 148 * sm_mhz / 1e3
+    return {"ops_per_pose_eval": ops, "achieved_gops": achieved, "peak_gops": peak, "frac": achieved / peak,
+            "peak_source": "nominal 16 MUFU results per clock per SM x 148 SMs x sampled SM clock",
+            "count": "pair loop only (4 per ligand atom x padded point); the sparse H-bond ex2 and KDE are extra"}
 
 
 def _pct(x, q):
@@ -587,7 +604,9 @@ def run_ours(args) -> None:
                          "kernel": "gd::mc_kernel (batched Monte Carlo, 50 steps x 3520 replicas per launch)",
                          "flops_per_pose_eval": fpp, "avg_launch_ms": avg_launch_ms,
                          "peak_source": "measured this run: FP32 FMA microbenchmark gd_fp32_peak (2 flops/FMA); "
-                                        "MEASURED_PEAKS.json has no FP32 figure"},
+                                        "MEASURED_PEAKS.json has no FP32 figure",
+                         "mufu": _mufu_share(len(job.lig_type), len(pk.type), n_rep * spi / (avg_launch_ms / 1e3),
+                                             ck.get("sm_mhz"))},
             "plain_kernel": {"value": plain_value, "unit": UNIT, "speedup_batched_over_plain": value / world / plain_value,
                              "launch": "all replicas in one launch (the reference's Dock launch structure)"},
             "plain_one_replica_per_launch": {**plain_one,
