@@ -103,6 +103,41 @@ def test_dock_drop_in_records(lib, enepara, oracle_lib):
     assert np.all(work[0]["replica"]["is_accept"][:n] == ref[0]["replica"]["is_accept"][:n])
 
 
+def test_acceptance_and_best_energy_statistics(lib, enepara, oracle_lib):
+    """Over every replica of a 96-replica ensemble (chains that diverged after a
+    flipped decision included): acceptance rates and best-energy distributions
+    of the GPU and the FP64 oracle agree statistically, and acceptance rises
+    with temperature."""
+    from scipy.stats import ks_2samp
+
+    temps = (0.3, 0.45, 0.7, 1.0, 1.5, 2.2, 3.3, 5.0)
+    cx = _small_ensemble(enepara, seed=17, nlig=4, nprt=3, temps=temps)
+    cx[0]["mcpara"]["steps_total"] = 200
+    cx[0]["mcpara"]["steps_per_dump"] = 200
+    n = int(cx[0]["size"]["n_rep"])
+    ref = cx.copy()
+    rrec = Lo.aligned_zeros(Lo.RECORD, n)
+    oracle_lib.montecarlo(ref, rrec, 0, 1, 23)
+    oracle_lib.montecarlo(ref, rrec, 0, 200, 23)
+    work = cx.copy()
+    with dock.DockSession(1, seed=23) as s:
+        rec = s.dock(work)
+
+    def summary(records):
+        acc = np.array([int(r["next_entry"]) for r in records], np.float64)   # accepted states + the initial one
+        best = np.array([r["replica"][:int(r["next_entry"])]["energy"][:, 9].min() for r in records], np.float64)
+        return acc, best
+
+    acc_g, best_g = summary(rec[:n])
+    acc_o, best_o = summary(rrec[:n])
+    se = np.sqrt(acc_g.var() / n + acc_o.var() / n) + 1e-9
+    assert abs(acc_g.mean() - acc_o.mean()) <= 3 * se, (acc_g.mean(), acc_o.mean(), se)
+    assert ks_2samp(best_g, best_o).pvalue > 0.01
+    tmp = work[0]["replica"]["idx_tmp"][:n]
+    by_t = [acc_g[tmp == t].mean() for t in range(len(temps))]
+    assert by_t[-1] > by_t[0], by_t
+
+
 def test_dock_initial_energy_record(lib, enepara, oracle_lib):
     """With one dump chunk, Record entry 0 is the initial state at step 0 -- the
     entry the reference prints as its known-answer line (kernel_print.C:9-15)."""
