@@ -61,11 +61,11 @@ __host__ __device__ inline float4 tab4_entry(float p1a, float p2a, float pmf0, f
 }
 __host__ __device__ inline float4 tab4_padding() { return make_float4(INFINITY, 0.f, 0.f, 0.f); }
 
+// The scalar parameters come first and the per-type tables last: the FP32
+// batched kernel stages only the scalar prefix in shared memory (it reads the
+// tables from global memory once per work item to build its per-atom-pair
+// tables); the FP64 and plain kernels stage the whole struct.
 struct alignas(16) DevParams {
-  float4 tab4[kLigTypes][kTabCols];   // 1/p1a, -p2a/p1a, -pmf0, pmf1 (tab4_entry); the point-type
-                                      // padding columns (>= 30) give exactly zero for every term
-  float2 tab2[kLigTypes][kTabCols];   // hdb1*c, -hdb0*hdb1*c with c = sqrt(log2(e)/2);
-                                      // zero where hdb0 <= 0.1 (no hydrogen-bond parameters)
   uint32_t hdbmask[kLigTypes];        // bit pt set where (ligand type, point type) has hdb0 > 0.1
   float hpl0[kLigTypes], hpl1[kLigTypes], hpl2[kLigTypes];
   float a_para[12], b_para[12], w[12];
@@ -76,8 +76,15 @@ struct alignas(16) DevParams {
   float move_scale[6];
   float kde3;                         // (h sqrt(2 pi))^3: the FP64 kernels divide by it
   float pad_;
+  float4 tab4[kLigTypes][kTabCols];   // 1/p1a, -p2a/p1a, -pmf0, pmf1 (tab4_entry); the point-type
+                                      // padding columns (>= 30) give exactly zero for every term
+  float2 tab2[kLigTypes][kTabCols];   // hdb1*c, -hdb0*hdb1*c with c = sqrt(log2(e)/2);
+                                      // zero where hdb0 <= 0.1 (no hydrogen-bond parameters)
 };
 static_assert(sizeof(DevParams) % 16 == 0, "DevParams must be a multiple of 16 bytes");
+// bytes of the scalar prefix (a multiple of 16: tab4 is 16-byte aligned)
+constexpr size_t kParamScalarBytes = offsetof(DevParams, tab4);
+static_assert(kParamScalarBytes % 16 == 0, "the scalar prefix is bulk-copied");
 
 // Per-replica running statistics, accumulated on the device in FP64.
 struct alignas(16) RepStats {

@@ -7,10 +7,11 @@
 // (src/backend_gpu/kernel_cuda_l1_montecarlo.cu:284-527).  Here one warp owns
 // one replica for a whole chunk of steps: the step needs no block barrier,
 // only warp shuffles.  A CTA holds R replica-warps that share one protein
-// conformation; per work item the CTA stages the force-field tables and the
-// KDE points (and, when it pays, the conformation itself) into shared memory
-// with 1-D bulk (TMA) copies, and its replica-warps read them every step.  A
-// persistent grid takes work items from an atomic queue, heaviest first.
+// conformation; per work item the CTA stages the force-field parameters and
+// the KDE points (and, when it pays, the conformation itself) into shared
+// memory with 1-D bulk (TMA) copies, and its replica-warps read them every
+// step.  A persistent grid takes work items from an atomic queue, heaviest
+// first.
 //
 // Pair loop, pass 1 (every term but the hydrophobic contact).  Lane i holds
 // pocket points row+i+32j (j < KPL) in registers.  The FP32 ligand sits in
@@ -90,8 +91,8 @@ __host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots,
 {
   SmemLayout s;
   uint32_t off = 0;
-  s.params = off;
-  off = align16(off + (uint32_t)sizeof(DevParams));
+  s.params = off;  // FP64: the whole DevParams; FP32: its scalar prefix
+  off = align16(off + (uint32_t)(fp64 ? sizeof(DevParams) : kParamScalarBytes));
   s.lgrp = off;
   off = align16(off + (uint32_t)sizeof(int2) * kMaxAtoms);
   s.pos = off;
@@ -235,8 +236,8 @@ struct PairAccP {
 };
 
 // Per work item, shared-memory tables of the atom-pair pair loop, built from
-// the per-type tables: for pair i (atoms a = 2i, b = 2i + 1) and point type pt,
-// e = i * kTabCols + pt,
+// the per-type tables (read from global memory): for pair i (atoms a = 2i,
+// b = 2i + 1) and point type pt, e = i * kTabCols + pt,
 //   apt[2e]     = (1/p1a, -p2a/p1a) of a and b interleaved: (a.x, b.x, a.y, b.y)
 //   apt[2e + 1] = (-pmf0, pmf1) interleaved
 //   aph[e]      = (hdb1 c, -hdb0 hdb1 c) interleaved
@@ -513,7 +514,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         T tps[KPL];
   #pragma unroll
         for (int j = 0; j < KPL; ++j) {
-          t4[j] = par->tab4[lt][pt[j]];
+          t4[j] = (PREC == kFP64 ? par : J.par)->tab4[lt][pt[j]];  // FP32 stages no tables
           if constexpr (PREC == kFP64) rf[j] = __ldg(J.ref4 + lt * kTabCols + pt[j]);
           else rf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
           t2[j] = make_float2(0.f, 0.f);
@@ -522,7 +523,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         if constexpr (PREC != kFP64) {
           if (any_hdb) {
   #pragma unroll
-            for (int j = 0; j < KPL; ++j) t2[j] = par->tab2[lt][pt[j]];
+            for (int j = 0; j < KPL; ++j) t2[j] = J.par->tab2[lt][pt[j]];
           }
         }
         if (any_psp) {
@@ -773,10 +774,11 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
   const bool pocket_in_smem = A.P > 0;
   if (threadIdx.x == 0) {
     fence_proxy_async_smem();
-    uint32_t bytes = (uint32_t)sizeof(DevParams) + (pocket_in_smem ? 24u * (uint32_t)P : 0u);
+    const uint32_t pbytes = (uint32_t)(FP64 ? sizeof(DevParams) : kParamScalarBytes);
+    uint32_t bytes = pbytes + (pocket_in_smem ? 24u * (uint32_t)P : 0u);
     if (kde_in_smem) bytes += 16u * (uint32_t)J.nkde;
     mbar_expect_tx(bar, bytes + A.stall_bytes);
-    bulk_g2s(smem + sl.params, J.par, (uint32_t)sizeof(DevParams), bar);
+    bulk_g2s(smem + sl.params, J.par, pbytes, bar);
     if (pocket_in_smem) {
       bulk_g2s(smem + sl.pos, J.pos + (size_t)wi.prt * P, 16u * (uint32_t)P, bar);
       bulk_g2s(smem + sl.aux, J.aux + (size_t)wi.prt * P, 8u * (uint32_t)P, bar);
@@ -829,9 +831,9 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         return;
       }
       if constexpr (PREC != kFP64 && KPL % 2 == 0) {
-        __syncthreads();  // parameters and type groups are in shared memory
+        __syncthreads();  // type groups are in shared memory
         if (wi.job != prev_job)
-          build_pair_tables(J.natom, reinterpret_cast<const DevParams *>(smem + sl.params),
+          build_pair_tables(J.natom, J.par,
                             reinterpret_cast<const int2 *>(smem + sl.lgrp), reinterpret_cast<float4 *>(smem + sl.apt),
                             reinterpret_cast<float4 *>(smem + sl.aph), reinterpret_cast<int4 *>(smem + sl.ahd));
       }
@@ -843,6 +845,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     const float4 *aph = reinterpret_cast<const float4 *>(smem + sl.aph);
     const int4 *ahd = reinterpret_cast<const int4 *>(smem + sl.ahd);
 
+    // FP32: only the scalar prefix of DevParams is in shared memory (no table is read through par)
     const DevParams *par = reinterpret_cast<const DevParams *>(smem + sl.params);
     // the protein conformation: staged in shared memory, or read through L1
     const float4 *pos = A.P > 0 ? reinterpret_cast<const float4 *>(smem + sl.pos)
