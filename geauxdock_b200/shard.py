@@ -1,5 +1,6 @@
-"""One process per GPU (torchrun): each rank runs its shard of a Complex's
-replicas and rank 0 gathers the final replica states.
+"""One process per GPU (torchrun), on one node or several: each rank runs its
+shard of a Complex's replicas and rank 0 gathers the final replica states; or,
+for many complexes, ranks take whole complexes from a shared queue.
 
 The shard of rank g of N is SetParaT's split (src/backend_gpu/prepair.C:366-392),
 cut at protein-conformation blocks when replica exchange is on, so exchange
@@ -8,6 +9,15 @@ collective.  Philox counters use the global replica index, so with one seed on
 every rank each replica's trajectory does not depend on N.  The only
 collective is the gather of the results at the end (NCCL between GPUs, gloo
 on CPU).
+
+Many complexes (the reference's MPI screening, src/main_mpi/server.C:27-66 and
+client_gpu.C): the reference's rank 0 hands the next complex to whichever
+client asks, and each client docks it with Dock.  Here every rank, rank 0
+included, claims the next complex index from one counter in a key-value store
+that all ranks share (a torch.distributed Store: TCPStore across nodes,
+FileStore or HashStore for tests), docks it on its own GPU through the drop-in
+Dock, and the results meet on rank 0 in one gather.  No rank only dispatches,
+and there is no MPI.
 """
 
 from __future__ import annotations
@@ -65,3 +75,55 @@ def gather_replicas(local: np.ndarray, device=None) -> np.ndarray | None:
         return None
     out = [p[:int(s.item())].cpu().numpy() for p, s in zip(parts, sizes)]
     return np.concatenate(out).view(Lo.REPLICA)
+
+
+def complex_seed(seed: int, index: int) -> int:
+    """The RNG seed of complex `index` in a queue seeded with `seed`: a complex's
+    result does not depend on which rank docks it or in what order."""
+    return (seed + 0x9E3779B97F4A7C15 * (index + 1)) & 0xFFFFFFFFFFFFFFFF
+
+
+def claim_jobs(store, n_jobs: int, key: str = "gd_next_complex"):
+    """Yield the indices this rank claims, one at a time, from the counter `key`
+    in `store`, until all n_jobs are taken.  Every index goes to exactly one rank;
+    a fast rank simply claims more (the reference's idle client asking the server)."""
+    while True:
+        i = int(store.add(key, 1)) - 1
+        if i >= n_jobs:
+            return
+        yield i
+
+
+def dock_queue(complexes, seed: int, store, key: str = "gd_next_complex") -> dict:
+    """Dock the complexes this rank claims from the shared counter on this
+    process's GPU (the library's `device_base` option selects it) through
+    SetParaT / CopyH2D / Dock, each with RNG seed complex_seed(seed, index).
+    Returns {index: final replica states of that complex}."""
+    from .dock import DockSession
+
+    out = {}
+    with DockSession(1) as s:
+        for i in claim_jobs(store, len(complexes), key):
+            cx = complexes[i].copy()
+            s.seed(complex_seed(seed, i))
+            s.dock(cx)
+            out[i] = cx[0]["replica"][:int(cx[0]["size"]["n_rep"])].copy()
+    return out
+
+
+def gather_results(local: dict) -> dict | None:
+    """Every rank's {index: result} merged on rank 0 (None elsewhere), in one
+    all_gather_object of the process group."""
+    import torch.distributed as dist
+
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, local)
+    if dist.get_rank() != 0:
+        return None
+    merged = {}
+    for part in parts:
+        for i, r in part.items():
+            if i in merged:
+                raise RuntimeError(f"complex {i} docked twice")
+            merged[i] = r
+    return dict(sorted(merged.items()))

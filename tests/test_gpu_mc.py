@@ -341,3 +341,29 @@ def test_bounded_wait_reports_timeout(lib, enepara):
         ens.run(20, 10)
         ens.sync()
         assert np.isfinite(ens.replicas(0)["energy"][:int(cx[0]["size"]["n_rep"])]).all()
+
+
+def test_complex_queue_matches_direct_dock(lib, enepara):
+    """The multi-complex queue (one process here, a HashStore counter): each
+    complex's result equals docking it alone with its derived seed, whatever
+    else the same Dock handle docked before it."""
+    import torch.distributed as dist
+
+    from geauxdock_b200 import shard
+
+    cxs = []
+    for k, (L, P) in enumerate([(14, 220), (23, 310), (9, 150)]):
+        rng = np.random.default_rng(40 + k)
+        pk = synth.make_pocket(rng, P, 2)
+        job = synth.make_job(rng, pk, L, 2, 60, 4, np.array([0.5, 1.0, 2.0], np.float32), seed=k)
+        cxs.append(synth.to_complex(job, pk, enepara, steps_total=200, steps_per_dump=100))
+    got = shard.dock_queue(cxs, 31, dist.HashStore())
+    assert sorted(got) == [0, 1, 2]
+    for i in (2, 0):
+        cx = cxs[i].copy()
+        with dock.DockSession(1, seed=0) as s:
+            s.seed(shard.complex_seed(31, i))
+            s.dock(cx)
+        want = cx[0]["replica"][:int(cx[0]["size"]["n_rep"])]
+        for f in want.dtype.names:                 # the fields; ReplicaMC's padding carries nothing
+            assert got[i][f].tobytes() == want[f].tobytes(), (i, f)

@@ -109,3 +109,47 @@ def test_gloo_replica_shards_and_gather(world):
         assert np.all(full["step"][b:e] == r)
         assert np.array_equal(full["movematrix"][b:e], want["movematrix"][b:e])
         assert np.array_equal(full["idx_rep"][b:e], want["idx_rep"][b:e])
+
+
+def _queue_worker(rank, world, port, store_path, n_jobs, q):
+    import time
+
+    from geauxdock_b200 import shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        store = dist.FileStore(store_path, world)
+        local = {}
+        for i in shard.claim_jobs(store, n_jobs):
+            time.sleep(0.002 * (rank + 1))       # ranks of different speed
+            local[i] = (rank, i * i)            # stands in for docking complex i
+        merged = shard.gather_results(local)
+        q.put((rank, len(local), merged))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [3])
+def test_gloo_complex_queue(world, tmp_path):
+    """Ranks claim complexes from one shared counter (the reference's MPI
+    server/client dispatch without a dispatching rank): every complex is taken
+    exactly once, faster ranks take more, and the results meet on rank 0."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    n_jobs = 60
+    procs = [ctx.Process(target=_queue_worker, args=(r, world, port, str(tmp_path / "store"), n_jobs, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = {r: (n, m) for r, n, m in (q.get(timeout=10) for _ in range(world))}
+    assert sum(n for n, _ in got.values()) == n_jobs
+    merged = got[0][1]
+    assert list(merged) == list(range(n_jobs))
+    assert all(v[1] == i * i for i, v in merged.items())
+    assert {v[0] for v in merged.values()} == set(range(world))
+    assert all(got[r][1] is None for r in range(1, world))
