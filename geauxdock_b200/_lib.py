@@ -34,7 +34,7 @@ GD_PREC_FP64 = 2
 # Every extern "C" symbol include/gdock.h declares.
 EXPORTED = [
     "gd_last_error", "gd_set_ngpu", "gd_get_ngpu",
-    "SetDevice", "DeviceAlloc", "DeviceFree", "SetParaT", "CopyH2D", "InitCurand", "gd_rng_seed", "Dock",
+    "SetDevice", "DeviceAlloc", "DeviceFree", "SetParaT", "CopyH2D", "InitCurand", "gd_rng_seed", "gd_rng_dock_reuse", "Dock",
     "gd_set_option", "gd_get_option", "gd_eval_poses",
     "gd_ensemble_create", "gd_ensemble_create_complex", "gd_ensemble_init", "gd_ensemble_run",
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
@@ -152,7 +152,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_set_ngpu": (i, [i]), "gd_get_ngpu": (i, []),
         "SetDevice": (i, []), "DeviceAlloc": (i, [vp, vp, vp]), "DeviceFree": (i, [vp, vp, vp]),
         "SetParaT": (i, [vp, vp]), "CopyH2D": (i, [vp, vp, vp]), "InitCurand": (i, [vp]),
-        "gd_rng_seed": (i, [vp, C.c_uint64]), "Dock": (i, [vp, vp, vp, vp, vp, vp]),
+        "gd_rng_seed": (i, [vp, C.c_uint64]), "gd_rng_dock_reuse": (i, [vp, vp, vp]), "Dock": (i, [vp, vp, vp, vp, vp, vp]),
         "gd_set_option": (i, [C.c_char_p, ll]), "gd_get_option": (ll, [C.c_char_p]),
         "gd_eval_poses": (i, [vp, i, vp, vp, i, vp, vp, vp]),
         "gd_ensemble_create": (i, [vp, i, vp, i, vp, i, vp]),

@@ -50,6 +50,14 @@ Options opts()
   return g_opt;
 }
 
+// Field by field: Options has padding, whose bytes a copy need not keep.
+bool same_options(const Options &a, const Options &b)
+{
+  return a.kernel == b.kernel && a.precision == b.precision && a.warps == b.warps && a.kpl == b.kpl &&
+         a.ab == b.ab && a.graph == b.graph && a.stage == b.stage && a.dock_cache == b.dock_cache &&
+         a.device_base == b.device_base && a.wait_limit == b.wait_limit && a.stall_test == b.stall_test;
+}
+
 constexpr size_t kSmemLimit = 227 * 1024;
 constexpr int kExchTag = 1;
 
@@ -61,6 +69,8 @@ struct gd_rng {
   uint64_t seed = 0;
   uint64_t calls = 0;
   int seeded = 0;
+  uint64_t dock_calls = 0;   // Dock calls on this handle's GPU
+  uint64_t dock_reused = 0;  // of them, refills of the kept device state
   // Dock's resident state on this handle's GPU, kept between calls and refilled
   // in place when the next Complex has the same shapes
   gd_ensemble *dock = nullptr;
@@ -489,7 +499,8 @@ int dock_ensemble(gd_rng *h, const Complex *c, int rb, int re, uint64_t seed, Re
   const Options o = opts();
   const size_t prt_bytes = sizeof(Protein) * (size_t)std::max(0, std::min(c->size.n_prt, GD_MAX_CONF_PRT));
   gd_ensemble *e = h->dock;
-  if (e && e->device == device && std::memcmp(&h->dock_opt, &o, sizeof(Options)) == 0 && e->jobs.size() == 1) {
+  ++h->dock_calls;
+  if (e && e->device == device && same_options(h->dock_opt, o) && e->jobs.size() == 1) {
     Tracer tr("refill");
     GD_TRY(set_device(device));
     GD_CUDA(cudaStreamSynchronize(e->st));
@@ -536,6 +547,7 @@ int dock_ensemble(gd_rng *h, const Complex *c, int rb, int re, uint64_t seed, Re
       e->ev_used = 0;
       e->launches = 0;
       e->all_launches = 0;
+      ++h->dock_reused;
       *out = e;
       return GD_OK;
     }
@@ -776,6 +788,14 @@ int InitCurand(gd_rng_t **rng)
     }
     rng[g]->calls = 0;
   }
+  return GD_OK;
+}
+
+int gd_rng_dock_reuse(const gd_rng_t *rng, uint64_t *calls, uint64_t *reused)
+{
+  if (!rng || !calls || !reused) return fail(GD_E_INVALID, "null argument");
+  *calls = rng->dock_calls;
+  *reused = rng->dock_reused;
   return GD_OK;
 }
 

@@ -40,6 +40,12 @@ class DockSession:
         for g in range(self.n):
             check(self.lib.gd_rng_seed(self.rng[g], seed + g))
 
+    def reuse(self, g: int = 0) -> tuple[int, int]:
+        """(Dock calls, calls that refilled the kept device state) of GPU g's handle."""
+        calls, reused = C.c_uint64(), C.c_uint64()
+        check(self.lib.gd_rng_dock_reuse(self.rng[g], C.byref(calls), C.byref(reused)))
+        return calls.value, reused.value
+
     def dock(self, cx: np.ndarray, record: np.ndarray | None = None) -> np.ndarray:
         """Dock one Complex record in place; returns the Record array (last dump chunk)."""
         assert cx.dtype == Lo.COMPLEX

@@ -70,6 +70,11 @@ int CopyH2D(Complex *ch, Complex **cd, ParaT **pt);
 int InitCurand(gd_rng_t **rng);
 /* Fix the seed of one handle (reproducible runs); resets its call counter. */
 int gd_rng_seed(gd_rng_t *rng, uint64_t seed);
+/* Dock calls made with this handle and how many of them refilled the device
+ * state kept from the previous call (same shapes and options) instead of
+ * rebuilding it.  No counterpart in the reference (it allocates once in
+ * DeviceAlloc and re-copies the whole Complex per call). */
+int gd_rng_dock_reuse(const gd_rng_t *rng, uint64_t *calls, uint64_t *reused);
 /* src/backend_gpu/backend_gpu.h:6-11 -- initial energy (forced accept), then
  * steps_total MC steps in chunks of steps_per_dump; after each chunk the
  * replicas' Record entries are copied to rh[rep_begin..rep_end].  Final

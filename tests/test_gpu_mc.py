@@ -291,6 +291,9 @@ def test_dock_reuses_device_state(lib, enepara):
                     w = cx.copy()
                     rec = s.dock(w)
                     res.append(written(w, rec, int(cx[0]["size"]["n_rep"])))
+                # calls 2 and 3 keep the shapes (new ligand; new protein of the same
+                # shape) and refill the kept state; call 4 changes them
+                assert s.reuse() == (4, 2 if cache else 0)
             out[cache] = res
     finally:
         check(lib.gd_set_option(b"dock_cache", 1))
