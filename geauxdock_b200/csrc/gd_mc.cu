@@ -570,35 +570,29 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     const int rows = ((J.ncdc[iprt] + 32 * KPL - 1) / (32 * KPL)) * (32 * KPL);
     for (int a0 = 0; a0 < L; a0 += AB) {
       T hpc[AB];
+      if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+        // atom-pair form, the same operations per component: h2[k] holds the
+        // sums of atoms a0 + 2k and a0 + 2k + 1 (AB is even)
+        const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f), c2 = f2(-0.5f / 81.0f);
+        float2 h2[AB / 2];
 #pragma unroll
-      for (int k = 0; k < AB; ++k) hpc[k] = 0;
-      for (int row = 0; row < rows; row += 32 * KPL) {
-        T px[KPL], py[KPL], pz[KPL], ph[KPL];
-#pragma unroll
-        for (int j = 0; j < KPL; ++j) {
-          const int p = row + 32 * j + lane;
-          const float4 q = pos[p];
-          px[j] = q.x; py[j] = q.y; pz[j] = q.z;
-          ph[j] = aux[p].x;
-        }
-        if constexpr (PREC != kFP64 && KPL % 2 == 0) {
-          // atom-pair form, the same operations per component: hpc[2k] and
-          // hpc[2k+1] are atoms a0 + 2k and a0 + 2k + 1 (AB is even)
-          const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f), c2 = f2(-0.5f / 81.0f);
+        for (int k = 0; k < AB / 2; ++k) h2[k] = f2(0.0f);
+        for (int row = 0; row < rows; row += 32 * KPL) {
           float2 npx[KPL], npy[KPL], npz[KPL], ph2[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
-            npx[j] = f2(-px[j]);
-            npy[j] = f2(-py[j]);
-            npz[j] = f2(-pz[j]);
-            ph2[j] = f2(ph[j]);
+            const int p = row + 32 * j + lane;
+            const float4 q = pos[p];
+            npx[j] = f2(-q.x);
+            npy[j] = f2(-q.y);
+            npz[j] = f2(-q.z);
+            ph2[j] = f2(aux[p].x);
           }
 #pragma unroll
           for (int k = 0; k < AB / 2; ++k) {
             const int a = a0 + 2 * k;
             if (a >= L) break;
             const LigPair la = lig[a >> 1];
-            float2 h2 = make_float2(hpc[2 * k], hpc[2 * k + 1]);
 #pragma unroll
             for (int j = 0; j < KPL; ++j) {
               const float2 dx = __fadd2_rn(la.x, npx[j]), dy = __fadd2_rn(la.y, npy[j]), dz = __fadd2_rn(la.z, npz[j]);
@@ -608,31 +602,46 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
               t.y = fmaxf(t.y, 0.0f);
               const float2 u = __ffma2_rn(d2, c2, one);
               const float2 w = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, t), t), u);
-              h2 = __ffma2_rn(ph2[j], w, h2);
+              h2[k] = __ffma2_rn(ph2[j], w, h2[k]);
             }
-            hpc[2 * k] = h2.x;
-            hpc[2 * k + 1] = h2.y;
           }
-          continue;
         }
 #pragma unroll
-        for (int k = 0; k < AB; ++k) {
-          const int a = a0 + k;
-          if (a >= L) break;
-          const V4<T> la = atom_at(lig, a);
+        for (int k = 0; k < AB / 2; ++k) {
+          hpc[2 * k] = h2[k].x;
+          hpc[2 * k + 1] = h2[k].y;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < AB; ++k) hpc[k] = 0;
+        for (int row = 0; row < rows; row += 32 * KPL) {
+          T px[KPL], py[KPL], pz[KPL], ph[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
-            const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
-            const T d2 = dx * dx + dy * dy + dz * dz;
-            T t, u;
-            if constexpr (PREC == kFP64) {
-              t = fmax(1.0 - d2 / 81.0, 0.0);
-              u = 1.0 - 0.5 * d2 / 81.0;
-            } else {
-              t = fmaxf(fmaf(d2, -1.0f / 81.0f, 1.0f), 0.0f);
-              u = fmaf(d2, -0.5f / 81.0f, 1.0f);
+            const int p = row + 32 * j + lane;
+            const float4 q = pos[p];
+            px[j] = q.x; py[j] = q.y; pz[j] = q.z;
+            ph[j] = aux[p].x;
+          }
+#pragma unroll
+          for (int k = 0; k < AB; ++k) {
+            const int a = a0 + k;
+            if (a >= L) break;
+            const V4<T> la = atom_at(lig, a);
+#pragma unroll
+            for (int j = 0; j < KPL; ++j) {
+              const T dx = la.x - px[j], dy = la.y - py[j], dz = la.z - pz[j];
+              const T d2 = dx * dx + dy * dy + dz * dz;
+              T t, u;
+              if constexpr (PREC == kFP64) {
+                t = fmax(1.0 - d2 / 81.0, 0.0);
+                u = 1.0 - 0.5 * d2 / 81.0;
+              } else {
+                t = fmaxf(fmaf(d2, -1.0f / 81.0f, 1.0f), 0.0f);
+                u = fmaf(d2, -0.5f / 81.0f, 1.0f);
+              }
+              hpc[k] += ph[j] * (t * t * t * u);
             }
-            hpc[k] += ph[j] * (t * t * t * u);
           }
         }
       }
