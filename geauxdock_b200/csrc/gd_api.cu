@@ -1282,6 +1282,9 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   for (int stage = can_stage ? 1 : 0; stage >= 0; --stage)
   for (const auto &sh : shapes) {
     if (e->precision == GD_PREC_FP64 && !(sh[0] == 1 && sh[1] == 8)) continue;
+    // FP32: kpl 1 is the per-type-group scalar loop, which the atom-pair loop of
+    // the even kpl shapes outruns on every workload measured; not worth tuning time
+    if (e->precision != GD_PREC_FP64 && sh[0] == 1) continue;
     for (int w : warps) {
       if (rc != GD_OK) break;
       TileConfig tc{w, sh[0], sh[1], stage};

@@ -370,3 +370,22 @@ def test_complex_queue_matches_direct_dock(lib, enepara):
         want = cx[0]["replica"][:int(cx[0]["size"]["n_rep"])]
         for f in want.dtype.names:                 # the fields; ReplicaMC's padding carries nothing
             assert got[i][f].tobytes() == want[f].tobytes(), (i, f)
+
+
+def test_autotune_restores_state_and_runs(lib, enepara, oracle_lib):
+    """The tile autotuner times candidate shapes on a snapshot of the replica
+    state and restores it: the tuned ensemble then follows the oracle's
+    trajectories.  FP32 candidates are the atom-pair shapes (even kpl)."""
+    cx = _small_ensemble(enepara, seed=29)
+    n = int(cx[0]["size"]["n_rep"])
+    ref = _oracle_run(oracle_lib, cx, 8, 60)
+    with dock.Ensemble.from_complexes([cx], [8]) as ens:
+        ens.init()
+        rep = ens.autotune(20)
+        ens.run(60)
+        ens.sync()
+        got = ens.replicas(0)
+    lines = rep.strip().splitlines()
+    assert lines[-1].startswith("chosen:") and len(lines) > 2
+    assert all("kpl=1 " not in l for l in lines[:-1])
+    assert _same_trajectory(got, ref[0]["replica"][:n]).mean() >= 0.9
