@@ -59,7 +59,6 @@ bool same_options(const Options &a, const Options &b)
 }
 
 constexpr size_t kSmemLimit = 227 * 1024;
-constexpr int kExchTag = 1;
 
 }  // namespace
 

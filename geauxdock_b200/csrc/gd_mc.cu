@@ -49,13 +49,6 @@ constexpr float kSqrt2PiInvNeg = -0.3989422804014327f;  // -1/sqrt(2 pi), kernel
 constexpr double kSqrt2PiInvNegD = -0.39894228040143267794;  // the same in FP64
 constexpr uint32_t kWaitLimit = 1u << 26;
 
-// hydrophobic contact polynomial 1 - (3.5/81 d2 - 4.5/81^2 d4 + 2.5/81^3 d6 - 0.5/81^4 d8)
-// (energy_prt_v1.cu:44-48), in Horner form in d2
-constexpr double kH1 = -3.5 / 81.0;
-constexpr double kH2 = 4.5 / (81.0 * 81.0);
-constexpr double kH3 = -2.5 / (81.0 * 81.0 * 81.0);
-constexpr double kH4 = 0.5 / (81.0 * 81.0 * 81.0 * 81.0);
-
 template <typename T>
 struct alignas(16) V4 {
   T x, y, z, w;
