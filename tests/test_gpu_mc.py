@@ -389,3 +389,34 @@ def test_autotune_restores_state_and_runs(lib, enepara, oracle_lib):
     assert lines[-1].startswith("chosen:") and len(lines) > 2
     assert all("kpl=1 " not in l for l in lines[:-1])
     assert _same_trajectory(got, ref[0]["replica"][:n]).mean() >= 0.9
+
+
+def test_empty_inputs(lib, enepara, oracle_lib):
+    """Zero poses, zero steps: no error and no change.  Dock with steps_total = 0
+    runs only the initial-energy step: every replica's energies are the oracle's
+    for its stored pose, and no Record is written (the reference copies Records
+    per dump chunk, backend_gpu.cu:63-133, and there is none)."""
+    cx = _small_ensemble(enepara, seed=31)
+    n = int(cx[0]["size"]["n_rep"])
+    out, raw, _ = dock.eval_poses(cx, np.zeros((0, 2), np.int32), np.zeros((0, 6), np.float32))
+    assert out.shape == (0, 10)
+    with dock.Ensemble.from_complexes([cx], [3]) as ens:
+        ens.init()
+        ens.sync()
+        before = ens.replicas(0).copy()
+        ens.run(0)
+        ens.sync()
+        after = ens.replicas(0)
+        for f in before.dtype.names:                # the fields; ReplicaMC's padding carries nothing
+            assert after[f].tobytes() == before[f].tobytes(), f
+        e0, _, _ = ens.eval_poses(0, np.zeros((0, 2), np.int32), np.zeros((0, 6), np.float32))
+        assert e0.shape == (0, 10)
+    work = cx.copy()
+    work[0]["mcpara"]["steps_total"] = 0
+    with dock.DockSession(1, seed=4) as s:
+        rec = s.dock(work)
+    got = work[0]["replica"][:n]
+    for r in range(0, n, 7):
+        want, _ = oracle_lib.energy(cx, int(got[r]["idx_lig"]), int(got[r]["idx_prt"]), cx[0]["replica"][r]["movematrix"])
+        _close(got[r]["energy"], want)
+        assert int(rec[r]["next_entry"]) == 0
