@@ -167,7 +167,9 @@ int configure(gd_ensemble *e, TileConfig tc)
     return fail(GD_E_INVALID, "replicas per CTA = %d outside [1, %d]", tc.warps_per_cta, kMaxCtaThreads / 32);
   // a pocket too large to stage is read through L1; KDE points that do not fit are read from global memory
   if (tc.stage && smem_for(e, tc.warps_per_cta, 0, 1) > kSmemLimit) tc.stage = 0;
-  e->Kst = e->Kmax;
+  // FP32 reads the KDE points through L1 (the shared memory left to L1 pays more than
+  // staging them); FP64 stages them
+  e->Kst = e->precision == GD_PREC_FP64 ? e->Kmax : 0;
   if (smem_for(e, tc.warps_per_cta, e->Kst, tc.stage) > kSmemLimit) e->Kst = 0;
   const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst, tc.stage);
   if (smem > kSmemLimit)
@@ -897,7 +899,7 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
   const Options o = opts();
   TileConfig tc{8, o.kpl, o.ab};
   if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
-  int kst = J.nkde;
+  int kst = precision == GD_PREC_FP64 ? J.nkde : 0;  // FP32: KDE points through L1
   int P = e->Pmax;
   if (kernel_smem_bytes(P, 0, e->lig_slots, tc.warps_per_cta, precision) > kSmemLimit) P = 0;  // through L1
   size_t smem = kernel_smem_bytes(P, kst, e->lig_slots, tc.warps_per_cta, precision);

@@ -705,6 +705,26 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   T macc = 0;
   {
     const int M = J.nmcs;
+    if (M <= 16) {
+      // two half-warps share each template: lane and lane + 16 take its even and odd atoms
+      const int m = lane & 15, h = lane >> 4;
+      T s = 0;
+      int n = 0;
+      if (m < M) {
+        for (int a = h; a < L; a += 2) {
+          const float4 q = J.mcs[(size_t)a * M + m];
+          if (q.w != 0.0f) {
+            const V4<T> la = atom_at(lig, a);
+            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+            s += dx * dx + dy * dy + dz * dz;
+            ++n;
+          }
+        }
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 16);
+      n += __shfl_xor_sync(0xffffffffu, n, 16);
+      if (m < M && h == 0) macc += (T)J.tcc[m] * sqrt(s / (T)n);
+    } else
     for (int m0 = 0; m0 < M; m0 += 32) {
       const int m = m0 + lane;
       if (m < M) {

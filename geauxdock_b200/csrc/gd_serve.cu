@@ -564,7 +564,7 @@ void gd_server_config_default(gd_server_config_t *cfg)
   cfg->max_replicas_per_job = 1024;
   cfg->max_atoms = kMaxAtoms;
   cfg->steps_per_round = 50;
-  cfg->kde_stage = 1024;
+  cfg->kde_stage = 0;  // FP32 reads the KDE points through L1
   cfg->warps = 0;
   cfg->device = 0;
 }

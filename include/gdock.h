@@ -274,7 +274,7 @@ typedef struct gd_server_config {
   int max_replicas_per_job; /* default 1024 */
   int max_atoms;            /* largest ligand accepted (sizes the per-warp buffers), default 128 */
   int steps_per_round;      /* MC steps between scheduling decisions, default 50 */
-  int kde_stage;            /* KDE points staged in shared memory (more: read from global), default 1024 */
+  int kde_stage;            /* KDE points staged in shared memory (more: read through L1), default 0 */
   int warps;                /* replicas per CTA, 0: occupancy model */
   int device;
 } gd_server_config_t;
