@@ -53,8 +53,8 @@ STEPS_PER_INTERVAL = 50
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:mc_kernel -s 4 -c 1
 #       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,2,8,0
-# (1,463,808 B read + 91,904 B written); it does not grow with the steps per launch.
-TRAFFIC_BYTES_PER_LAUNCH = 1_463_808 + 91_904
+# (1,465,856 B read + 45,056 B written); it does not grow with the steps per launch.
+TRAFFIC_BYTES_PER_LAUNCH = 1_465_856 + 45_056
 
 
 def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
