@@ -7,8 +7,8 @@
 // (src/backend_gpu/kernel_cuda_l1_montecarlo.cu:284-527).  Here one warp owns
 // one replica for a whole chunk of steps: the step needs no block barrier,
 // only warp shuffles.  A CTA holds R replica-warps that share one protein
-// conformation; per work item the CTA stages the force-field parameters and
-// the KDE points (and, when it pays, the conformation itself) into shared
+// conformation; per work item the CTA stages the force-field parameters (in
+// FP64 also the KDE points; when it pays, the conformation itself) into shared
 // memory with 1-D bulk (TMA) copies, and its replica-warps read them every
 // step.  A persistent grid takes work items from an atomic queue, heaviest
 // first.
