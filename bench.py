@@ -196,20 +196,25 @@ def cpu_reference_sample(cx, seconds: float) -> dict:
 
 
 def run_reference(args) -> None:
+    """The reference's own CPU Monte Carlo on the headline workload.  This
+    process never loads libgdock.so: the parameter tables come from the
+    reference's OptimizeEnepara, the Complex from the numpy generator, and the
+    line lists the in-tree libraries the process mapped."""
     rank, world, local = _dist()
     if rank != 0:
         return
     os.environ.setdefault("OMP_PROC_BIND", "true")
-    from geauxdock_b200 import layout as Lo, synth
+    from geauxdock_b200 import layout as Lo, params, synth
     from oracle import oracle as O
 
-    ep, pk, job = _workload(0)
-    cx = synth.to_complex(job, pk, ep, steps_per_exchange=STEPS_PER_INTERVAL)
-    n = int(cx[0]["size"]["n_rep"])
     if not O.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgdref.so not built: the reference "
                                                               "sources were absent when build() ran"}))
         return
+    ep = O.ref_optimize_enepara(params.default_enepara0())
+    pk, job = synth.config2(seed=1)
+    cx = synth.to_complex(job, pk, ep, steps_per_exchange=STEPS_PER_INTERVAL)
+    n = int(cx[0]["size"]["n_rep"])
     ref = O.ref()
     cores = os.cpu_count() or 1
     ref.gdref_set_threads(cores)
@@ -232,9 +237,10 @@ def run_reference(args) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, Astex-like shapes)",
-        "config": _config(n, 1, {"sample": sample}), "impl": "reference",
+        "config": _config(n, world), "impl": "reference", "sample": sample,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_loaded": O.mapped_libraries(ROOT)}))
 
 
 def _hbm_share(launch_ms: float) -> dict:
@@ -594,7 +600,8 @@ def run_ours(args) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, Astex-like shapes)",
-            "config": _config(n_rep, world, {"autotune": tune.strip().splitlines()[-1] if tune else "off"}),
+            "config": _config(n_rep, world),
+            "autotune": tune.strip().splitlines()[-1] if tune else "off",
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": Lo.COMPLEX.itemsize,
                     "d2h_bytes_per_step": Lo.RECORD.itemsize * n_rep + Lo.REPLICA.itemsize * n_rep,
                     "step": f"one Dock call: CopyH2D + initial energies + {e2e_steps} MC steps + Record copy",

@@ -27,7 +27,7 @@ struct Options {
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
   int device_base = 0;        // the drop-in API's GPU g is CUDA device device_base + g
-  long long wait_limit = 0;   // polls of a bounded shared-memory wait (0: the kernel's default)
+  long long wait_limit = 0;   // microseconds of a bounded shared-memory wait (0: one second)
   int stall_test = 0;         // test hook: staging barriers that never complete (bounded waits run out)
 };
 Options g_opt;

@@ -146,11 +146,29 @@ __device__ __forceinline__ void fence_proxy_async_smem()
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Bounded wait for phase `parity` of `bar` to complete.  Returns false after
-// `limit` polls instead of spinning forever.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit)
+// Nanoseconds of the GPU's global timer (%globaltimer).
+__device__ __forceinline__ uint64_t global_ns()
 {
-  for (uint32_t i = 0; i < limit; ++i) {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Remove `bytes` from the transaction count of the barrier's current phase
+// (bytes announced by expect_tx that no copy will deliver).
+__device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait for phase `parity` of `bar` to complete.  Returns false once
+// `limit_ns` nanoseconds of the global timer have passed instead of spinning
+// forever.  The result is per thread: a caller that must act on it as a CTA
+// combines it with __syncthreads_and.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+  const uint64_t t0 = global_ns();
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -160,8 +178,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
         : "r"(smem_addr(bar)), "r"(parity)
         : "memory");
     if (done) return true;
+    if (global_ns() - t0 > limit_ns) return false;
   }
-  return false;
 }
 
 }  // namespace gd

@@ -193,7 +193,7 @@ struct KArgs {
   int s_begin, nsteps, flags;
   const int *d_step;       // if set, steps start at *d_step + s_begin (graph replay)
   int P, Kst, lig_slots;   // smem layout (maxima over the launched jobs); P = 0: pocket read from global memory
-  uint32_t wait_limit;     // polls of a bounded shared-memory wait before it gives up (0: the default)
+  uint32_t wait_limit;     // microseconds a bounded shared-memory wait lasts before it gives up (0: one second)
   uint32_t stall_bytes;    // test hook: bytes announced to the staging barrier that no copy delivers, so
                            // that its bounded wait runs out (0 in normal use)
   // pose evaluation

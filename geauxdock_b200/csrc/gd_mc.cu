@@ -47,7 +47,10 @@ namespace {
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kSqrt2PiInvNeg = -0.3989422804014327f;  // -1/sqrt(2 pi), kernel_cuda_l1_montecarlo.cu:14
 constexpr double kSqrt2PiInvNegD = -0.39894228040143267794;  // the same in FP64
-constexpr uint32_t kWaitLimit = 1u << 26;
+// bound of the staging waits when the wait_limit option is 0: one second
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+__device__ __forceinline__ uint64_t wait_limit_ns(uint32_t us) { return us ? 1000ull * us : kWaitLimitNs; }
 
 template <typename T>
 struct alignas(16) V4 {
@@ -785,8 +788,9 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
 // ------------------------------------------------------------ kernels --
 
 
-// Stage the shared data of work item `wi` into shared memory.  Returns false
-// if the bulk copies did not complete within the wait limit.
+// Stage the shared data of work item `wi` into shared memory.  Returns false,
+// in every thread of the CTA alike, if the bulk copies did not complete within
+// the wait limit; the barrier phase is then left open (see stage_abandon).
 template <bool FP64>
 __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, unsigned char *smem,
                            const SmemLayout &sl, uint64_t *bar, uint32_t &phase)
@@ -809,9 +813,23 @@ __device__ bool stage_item(const KArgs &A, const DevJob &J, const WorkItem &wi, 
   }
   int2 *lg = reinterpret_cast<int2 *>(smem + sl.lgrp);
   for (int a = threadIdx.x; a < J.natom; a += blockDim.x) lg[a] = J.lgrp[a];
-  const bool ok = mbar_wait(bar, phase, A.wait_limit ? A.wait_limit : kWaitLimit);
+  // one decision for the whole CTA: a thread that saw the phase complete and
+  // one that gave up must not go separate ways
+  const bool ok = __syncthreads_and(mbar_wait(bar, phase, wait_limit_ns(A.wait_limit)) ? 1 : 0) != 0;
   phase ^= 1u;
   return ok;
+}
+
+// After stage_item gave up: before the CTA returns (and its shared memory goes
+// to another CTA), let the copies it issued land.  Bytes the test hook
+// announced without a copy are taken off the barrier first, so that the phase
+// completes exactly when the real copies have arrived; the wait is bounded
+// again.  `phase` is the parity stage_item already advanced.
+__device__ void stage_abandon(const KArgs &A, uint64_t *bar, uint32_t phase)
+{
+  if (threadIdx.x == 0 && A.stall_bytes) mbar_complete_tx(bar, A.stall_bytes);
+  __syncthreads();
+  (void)__syncthreads_and(mbar_wait(bar, phase ^ 1u, wait_limit_ns(A.wait_limit)) ? 1 : 0);
 }
 
 // Per-warp FP64 statistics kept in shared memory during a chunk (lane 0).
@@ -847,9 +865,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     if (wi.job != prev_job || wi.prt != prev_prt) {
       if (!stage_item<PREC == kFP64>(A, J, wi, smem, sl, &bar, phase)) {
         if (threadIdx.x == 0) atomicOr(A.err, kErrTimeout);
-        // the copies it issued complete whatever the barrier's count says; wait
-        // (bounded) for the phase once more before the CTA's shared memory goes
-        mbar_wait(&bar, phase ^ 1u, A.wait_limit ? A.wait_limit : kWaitLimit);
+        stage_abandon(A, &bar, phase);
         return;
       }
       if constexpr (PREC != kFP64 && KPL % 2 == 0) {

@@ -12,7 +12,7 @@
 // device layout of the Complex) in one fixed-size array declared below.
 //
 // The scratch array is a file-scope __device__ variable: every GPU that loads
-// libgdock.so holds it (about 5.6 MB) until the process exits.  Its size covers
+// libgdock.so holds it (gd_noalloc_scratch_bytes(): 5.60 MiB) until the process exits.  Its size covers
 // the reference Complex's own capacity (64 ligand atoms, 64 ligand
 // conformations, 20 protein conformations of up to 2048 points, 10240 KDE
 // points, 512 MCS rows); inputs beyond that are rejected with GD_E_CAPACITY.
@@ -437,11 +437,19 @@ extern "C" int gd_eval_poses_noalloc(const Complex *d_complex, int n, const int 
 {
   if (!d_complex || n < 0 || (n > 0 && (!d_conf || !d_mm || !d_out))) return fail(GD_E_INVALID, "null argument");
   if (precision < GD_PREC_FP32 || precision > GD_PREC_FP64) return fail(GD_E_INVALID, "precision = %d", precision);
-  NoAllocScratch *S = nullptr;
-  GD_TRY(noalloc_scratch(&S));
   cudaStream_t st = (cudaStream_t)stream;
   int nsm = 0, dev = 0;
   GD_CUDA(cudaGetDevice(&dev));
+  if (st != nullptr) {
+    // the scratch address below is the current device's: the stream must belong to it
+    int sdev = -1;
+    GD_CUDA(cudaStreamGetDevice(st, &sdev));
+    if (sdev != dev)
+      return fail(GD_E_INVALID, "gd_eval_poses_noalloc: the stream belongs to device %d, the current device is %d",
+                  sdev, dev);
+  }
+  NoAllocScratch *S = nullptr;
+  GD_TRY(noalloc_scratch(&S));
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   // the failure flag and its details must start at zero on every call
   GD_CUDA(cudaMemsetAsync(&S->err, 0, sizeof(int) * 4, st));

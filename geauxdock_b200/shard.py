@@ -94,16 +94,32 @@ def claim_jobs(store, n_jobs: int, key: str = "gd_next_complex"):
         yield i
 
 
+_queue_generation: dict = {}
+
+
+def queue_key(store, key: str) -> str:
+    """The counter key of this process's next queue on `store`: `key` with a
+    generation suffix.  Every rank calls dock_queue the same number of times
+    (it is collective, like gather_results), so the ranks agree on the
+    generation, and a second queue on the same store starts from 0 instead of
+    past the first queue's end."""
+    g = _queue_generation.get((id(store), key), 0)
+    _queue_generation[(id(store), key)] = g + 1
+    return f"{key}/{g}"
+
+
 def dock_queue(complexes, seed: int, store, key: str = "gd_next_complex") -> dict:
     """Dock the complexes this rank claims from the shared counter on this
     process's GPU (the library's `device_base` option selects it) through
     SetParaT / CopyH2D / Dock, each with RNG seed complex_seed(seed, index).
+    Collective: every rank calls it, once per queue.
     Returns {index: final replica states of that complex}."""
     from .dock import DockSession
 
     out = {}
+    qkey = queue_key(store, key)
     with DockSession(1) as s:
-        for i in claim_jobs(store, len(complexes), key):
+        for i in claim_jobs(store, len(complexes), qkey):
             cx = complexes[i].copy()
             s.seed(complex_seed(seed, i))
             s.dock(cx)
@@ -111,9 +127,10 @@ def dock_queue(complexes, seed: int, store, key: str = "gd_next_complex") -> dic
     return out
 
 
-def gather_results(local: dict) -> dict | None:
+def gather_results(local: dict, n_jobs: int | None = None) -> dict | None:
     """Every rank's {index: result} merged on rank 0 (None elsewhere), in one
-    all_gather_object of the process group."""
+    all_gather_object of the process group.  With n_jobs, rank 0 checks that
+    indices 0..n_jobs-1 all arrived, each once."""
     import torch.distributed as dist
 
     parts = [None] * dist.get_world_size()
@@ -126,4 +143,7 @@ def gather_results(local: dict) -> dict | None:
             if i in merged:
                 raise RuntimeError(f"complex {i} docked twice")
             merged[i] = r
+    if n_jobs is not None and sorted(merged) != list(range(n_jobs)):
+        missing = sorted(set(range(n_jobs)) - set(merged))
+        raise RuntimeError(f"{len(merged)} of {n_jobs} complexes gathered; missing {missing[:8]}")
     return dict(sorted(merged.items()))

@@ -104,8 +104,9 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
  * unchanged; 0: everything is rebuilt and freed per call), "device_base" (the
  * drop-in API's GPU g is CUDA device device_base + g, for one process per GPU;
  * set it before SetDevice/DeviceAlloc and keep it), "wait_limit"
- * (polls of the kernel's bounded shared-memory waits before they give up and
- * report GD_E_TIMEOUT; 0: the default), "stall_test" (test hook, 0 in normal
+ * (microseconds, on the GPU's global timer, that the kernel's bounded
+ * shared-memory waits last before they give up and report GD_E_TIMEOUT;
+ * 0: one second), "stall_test" (test hook, 0 in normal
  * use: ensembles announce bytes to their staging barriers that no copy
  * delivers, so that the bounded waits run out).  Applies to objects created
  * afterwards on the calling process. */
@@ -129,14 +130,17 @@ int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int
  * memory the caller owns: d_complex is a reference-layout Complex (for
  * example cd[g] after CopyH2D), d_conf[n][2] / d_mm[n][6] the poses,
  * d_out[n][10] and d_raw[n][9] (may be NULL) the energies; stream is a
- * cudaStream_t (NULL: the legacy default stream); the call returns after
- * the work on that stream finished.  The packed device layout goes into one
- * fixed scratch array in the library (gd_noalloc_scratch_bytes(), about
- * 5.6 MB, held on every GPU that loads the library until exit), sized for the
- * reference Complex's caps: larger sizes fail with GD_E_CAPACITY.  The first
- * call on a device looks up the scratch array's address; make that first
- * call before any stream capture.  All calls on a device share the scratch
- * array: calls whose GPU work overlaps race on it. */
+ * cudaStream_t of the calling thread's current device (NULL: its legacy
+ * default stream; a stream of another device is refused with GD_E_INVALID).
+ * The call is synchronous: it ends by copying a status word back and waiting
+ * for the stream, so it returns after its work on that stream finished.  The
+ * packed device layout goes into one fixed scratch array in the library
+ * (gd_noalloc_scratch_bytes(): 5.60 MiB, held on every GPU that loads the
+ * library until exit), sized for the reference Complex's caps: larger sizes
+ * fail with GD_E_CAPACITY.  The first call on a device looks up the scratch
+ * array's address (set-up); make that first call before any stream capture.
+ * All calls on a device share the scratch array, which keeps the last call's
+ * contents: calls whose GPU work overlaps race on it. */
 int gd_eval_poses_noalloc(const Complex *d_complex, int n, const int *d_conf, const float *d_mm, int precision,
                           float *d_out, float *d_raw, void *stream);
 size_t gd_noalloc_scratch_bytes(void);

@@ -28,8 +28,10 @@ def build(reference: str | None = None) -> None:
     import subprocess
 
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    ref = reference or os.environ.get("GD_REFERENCE", "/root/reference")
-    if Path(ref, "src").is_dir():
+    from oracle.refpath import reference_sources
+
+    ref = reference or reference_sources()
+    if ref is not None and Path(ref, "src").is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
 
 
@@ -65,10 +67,35 @@ def ref() -> C.CDLL:
         lib.gdref_sizeof.argtypes = [C.c_char_p]
         lib.gdref_sizeof.restype = C.c_size_t
         lib.gdref_load_enepara.argtypes = [C.c_char_p] * 4 + [vp, vp]
+        lib.gdref_optimize_enepara.argtypes = [vp, vp]
         lib.gdref_load_complex.argtypes = [C.c_char_p] * 8 + [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                                                C.c_int, C.c_int, vp]
         _ref = lib
     return _ref
+
+
+def ref_optimize_enepara(ep0: np.ndarray) -> np.ndarray:
+    """The reference's own OptimizeEnepara (util_optimize_soa.C:489-540) on a raw
+    EnePara0 record: an EnePara record, built without libgdock.so."""
+    from geauxdock_b200 import layout as Lo
+
+    src = np.array([ep0], dtype=Lo.ENEPARA0)
+    out = np.zeros(1, dtype=Lo.ENEPARA)
+    ref().gdref_optimize_enepara(src.ctypes.data, out.ctypes.data)
+    return out[0]
+
+
+def mapped_libraries(root: Path) -> list[str]:
+    """Shared objects under `root` that this process has mapped (/proc/self/maps)."""
+    out = set()
+    try:
+        for ln in Path("/proc/self/maps").read_text().splitlines():
+            f = ln.split()[-1] if ln.split() else ""
+            if f.endswith(".so") and f.startswith(str(root)):
+                out.add(str(Path(f).relative_to(root)))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 def energy(cx: np.ndarray, il: int, ip: int, mm) -> tuple[np.ndarray, np.ndarray]:

@@ -166,6 +166,14 @@ void gdref_load_enepara(const char *paras, const char *weight, const char *nor_a
   OptimizeEnepara(e0, (EnePara *)enepara_out);
 }
 
+// The reference's OptimizeEnepara (util_optimize_soa.C:489-540) on a raw
+// parameter set: the precomputed tables a Complex carries.
+void gdref_optimize_enepara(const void *enepara0, void *enepara_out)
+{
+  std::memset(enepara_out, 0, sizeof(EnePara));
+  OptimizeEnepara((EnePara0 *)enepara0, (EnePara *)enepara_out);
+}
+
 // One ligand (.sdf + .ff) against one protein (.pdb), assembled into a Complex
 // exactly as src/frontend/server1.C:52-217 does for complex i.  Returns the
 // number of replicas.

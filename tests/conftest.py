@@ -7,7 +7,10 @@ ROOT = Path(__file__).resolve().parents[1]
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-REFERENCE = Path("/root/reference")
+from oracle.refpath import reference_path, reference_sources  # noqa: E402
+
+# the reference project's root (GD_REFERENCE; see oracle/refpath.py)
+REFERENCE = reference_path()
 
 
 def pytest_configure(config):
@@ -40,4 +43,4 @@ def oracle_lib():
 
 
 def have_reference_sources() -> bool:
-    return (REFERENCE / "src").is_dir() and (REFERENCE / "data").is_dir()
+    return reference_sources() is not None

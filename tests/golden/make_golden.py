@@ -22,7 +22,9 @@ sys.path.insert(0, str(ROOT))
 from geauxdock_b200 import layout as Lo, params, synth  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+from oracle.refpath import reference_path  # noqa: E402
+
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else reference_path()
 
 
 def philox_kat():

@@ -32,3 +32,6 @@ def test_reference_arm_json_line(oracle_lib):
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # the reference arm runs the reference alone: none of this package's libraries is mapped
+    assert "oracle/_ref/libgdref.so" in d["libraries_loaded"]
+    assert not [f for f in d["libraries_loaded"] if f.startswith("geauxdock_b200/")], d["libraries_loaded"]

@@ -7,6 +7,7 @@ import pytest
 
 from geauxdock_b200 import dock, layout as Lo, synth
 from geauxdock_b200._lib import GD_E_INVALID, GdockError, check
+from oracle import tolerance as TOL
 
 pytestmark = pytest.mark.gpu
 
@@ -26,11 +27,11 @@ def _oracle_run(O, cx, seed, steps, spx=0, record=None):
     return ref
 
 
-def _close(a, b, tol=1e-5):
-    """Energies agree to tol in the terms' normalised scale: |a - b| <= tol * max(|b|, 1)."""
-    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
-    assert np.all(np.abs(a - b) <= tol * np.maximum(np.abs(b), 1.0)), float(
-        (np.abs(a - b) / np.maximum(np.abs(b), 1.0)).max())
+def _close(a, b, tol=TOL.REL):
+    """Energies agree within the parity tolerance (oracle/tolerance.py), with
+    tol in place of its 1e-5: |a - b| <= tol * max(|b|, tau_i) per term."""
+    s = TOL.scaled_error(a, b) * (TOL.REL / tol)
+    assert np.all(s <= 1.0), float(s.max())
 
 
 def _same_trajectory(got, want):
@@ -148,7 +149,7 @@ def test_dock_initial_energy_record(lib, enepara, oracle_lib):
     e, _ = oracle_lib.energy(cx, 0, 0, np.zeros(6, np.float32))
     first = rec[0]["replica"][0]
     assert first["step"] == 0 and rec[0]["next_entry"] >= 1
-    assert np.all(np.abs(first["energy"] - e) <= 1e-5 * np.maximum(np.abs(e), 1.0))
+    TOL.check(first["energy"], e, "initial energy record")
 
 
 def test_plain_kernel_matches_batched(lib, enepara):

@@ -120,12 +120,16 @@ def _queue_worker(rank, world, port, store_path, n_jobs, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         store = dist.FileStore(store_path, world)
-        local = {}
-        for i in shard.claim_jobs(store, n_jobs):
-            time.sleep(0.002 * (rank + 1))       # ranks of different speed
-            local[i] = (rank, i * i)            # stands in for docking complex i
-        merged = shard.gather_results(local)
-        q.put((rank, len(local), merged))
+        out = []
+        # two queues on one store, as dock_queue runs them: the second starts
+        # from index 0 again (its own generation of the counter key)
+        for gen in range(2):
+            local = {}
+            for i in shard.claim_jobs(store, n_jobs, shard.queue_key(store, "gd_next_complex")):
+                time.sleep(0.002 * (rank + 1))       # ranks of different speed
+                local[i] = (rank, i * i + gen)      # stands in for docking complex i
+            out.append((len(local), shard.gather_results(local, n_jobs)))
+        q.put((rank, out))
     finally:
         dist.destroy_process_group()
 
@@ -146,10 +150,27 @@ def test_gloo_complex_queue(world, tmp_path):
     for p in procs:
         p.join(120)
         assert p.exitcode == 0
-    got = {r: (n, m) for r, n, m in (q.get(timeout=10) for _ in range(world))}
-    assert sum(n for n, _ in got.values()) == n_jobs
-    merged = got[0][1]
-    assert list(merged) == list(range(n_jobs))
-    assert all(v[1] == i * i for i, v in merged.items())
-    assert {v[0] for v in merged.values()} == set(range(world))
-    assert all(got[r][1] is None for r in range(1, world))
+    res = dict(q.get(timeout=10) for _ in range(world))
+    for gen in range(2):
+        got = {r: res[r][gen] for r in range(world)}
+        assert sum(n for n, _ in got.values()) == n_jobs
+        merged = got[0][1]
+        assert list(merged) == list(range(n_jobs))
+        assert all(v[1] == i * i + gen for i, v in merged.items())
+        assert {v[0] for v in merged.values()} == set(range(world))
+        assert all(got[r][1] is None for r in range(1, world))
+
+
+def test_gather_results_rejects_missing():
+    """gather_results with n_jobs fails loudly when an index is missing
+    (one gloo rank)."""
+    from geauxdock_b200 import shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()))
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        assert list(shard.gather_results({0: 1, 1: 2}, 2)) == [0, 1]
+        with pytest.raises(RuntimeError, match="missing"):
+            shard.gather_results({0: 1, 2: 3}, 3)
+    finally:
+        dist.destroy_process_group()
