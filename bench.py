@@ -26,8 +26,12 @@ serving    the request loop under Poisson arrivals at 200 req/s and at 70 % of
 
 --workload ensemble|screening|serving runs one leg.  --impl reference runs the
 reference's CPU implementation instead (rank 0).
-Multi-GPU (torchrun): each rank runs its own ensemble (weak scaling, no
-data-path collective); timing is the max over ranks.
+Multi-GPU (torchrun): the headline is weak scaling -- each rank docks its own
+complex of the headline shape (independent objects, no data-path collective),
+timing the max over ranks.  The "partition" leg then splits ONE complex's
+replicas across the ranks with the library's own split (gd_replica_range, cut
+at protein-conformation blocks) and gathers every final replica on rank 0 over
+NCCL: strong scaling of the product's multi-GPU path, with the gather timed.
 """
 
 from __future__ import annotations
@@ -79,20 +83,27 @@ def _args():
     p.add_argument("--skip-extras", action="store_true",
                    help="only the timed batched kernel (for profiling): no plain kernel, e2e, CPU baseline, "
                         "screening or serving legs")
-    p.add_argument("--workload", choices=["all", "ensemble", "screening", "serving"], default="all",
-                   help="ensemble: the headline line only; screening / serving: that leg alone")
+    p.add_argument("--workload", choices=["all", "ensemble", "screening", "serving", "single"], default="all",
+                   help="ensemble: the headline line only; screening / serving / single: that leg alone")
+    p.add_argument("--single-steps", type=int, default=3000, help="MC steps of the single-replica leg")
     p.add_argument("--screen-ligands", type=int, default=512)
     p.add_argument("--screen-intervals", type=int, default=2)
     p.add_argument("--plain-ligands", type=int, default=48,
                    help="ligands of the screening set timed with the plain one-launch-per-ligand kernel")
     p.add_argument("--plain-replicas", type=int, default=16,
                    help="replicas of the ensemble timed with the plain kernel, one launch per replica")
-    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-requests", type=int, default=48,
+                   help="requests of the run at the named arrival rate (which also measures the capacity)")
+    p.add_argument("--serve-loads", default="0.7",
+                   help="comma-separated fractions of the measured capacity to run below-capacity streams at")
+    p.add_argument("--serve-load-requests", type=int, default=24, help="requests of each below-capacity stream")
     p.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     p.add_argument("--serve-steps", type=int, default=2000)
     p.add_argument("--serve-max-active", type=int, default=0,
                    help="replicas per serving round (0: the server's default, four waves of resident replicas)")
     p.add_argument("--serve-round", type=int, default=STEPS_PER_INTERVAL, help="MC steps per serving round")
+    p.add_argument("--partition-intervals", type=int, default=5,
+                   help="exchange intervals timed in the multi-GPU partition leg (one complex split across ranks)")
     return p.parse_args()
 
 
@@ -159,7 +170,7 @@ def _config(n_rep: int, world: int, extra: dict | None = None) -> dict:
                      "conformations, 400 KDE points, 16 MCS templates, 16 temperatures 0.3-3.0, exchange every "
                      f"{STEPS_PER_INTERVAL} steps",
          "replicas_per_gpu": n_rep, "mc_steps_per_bench_step": STEPS_PER_INTERVAL,
-         "parallelism": f"replica shards x{world} (independent ensembles per GPU)",
+         "parallelism": f"one complex per GPU x{world} (independent objects, no data-path collective)",
          "l2": "flushed between timed steps (256 MiB write)"}
     if extra:
         c.update(extra)
@@ -277,6 +288,61 @@ def _pct(x, q):
     return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
 
 
+def run_single(args, local: int) -> dict:
+    """The plain method's single complex: one 24-atom ligand, one 600-point
+    pocket, 200 KDE points, 8 MCS templates, one temperature, ONE replica,
+    3000 MC steps -- a latency workload (one replica is one warp of the batched
+    kernel, one CTA of the plain kernel).  Device time of the 3000 steps
+    (CUDA events), and the reference's own CPU Monte Carlo on the same replica
+    (a bounded sample of the steps; one replica occupies one thread)."""
+    import torch
+
+    from geauxdock_b200 import dock, layout as Lo, params, synth
+    from geauxdock_b200._lib import check, load
+
+    lib = load()
+    ep = params.optimize_enepara(params.default_enepara0())
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, ep, steps_total=args.single_steps, steps_per_dump=200)
+    out = {"workload": "1 complex: ligand 24 atoms, pocket 600 points, 200 KDE points, 8 MCS templates, "
+                       f"1 temperature, 1 replica, {args.single_steps} MC steps"}
+    for name, kern in (("batched", 0), ("plain", 1)):
+        check(lib.gd_set_option(b"kernel", kern))
+        try:
+            with dock.Ensemble.from_complexes([cx], [1]) as ens:
+                ens.init()
+                ens.run(200)                 # warm-up
+                ens.sync()
+                st = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                ens.run(args.single_steps)
+                b.record(st)
+                b.synchronize()
+                ens.sync()
+                ms = a.elapsed_time(b)
+        finally:
+            check(lib.gd_set_option(b"kernel", 0))
+        out[name] = {"value": args.single_steps / (ms / 1e3), "unit": UNIT, "ms": ms}
+    from oracle import oracle as O
+
+    if O.have_ref():
+        ref = O.ref()
+        ref.gdref_set_threads(1)
+        work = cx.copy()
+        rec = Lo.aligned_zeros(Lo.RECORD, 1)
+        ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, 1)
+        n = 200
+        t0 = time.perf_counter()
+        ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 0, n)
+        dt = time.perf_counter() - t0
+        ref.gdref_set_threads(os.cpu_count() or 1)
+        out["cpu_reference"] = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+                                "sample": f"{n} of the {args.single_steps} MC steps, reference MonteCarlo_d"}
+        out["speedup_batched_over_cpu"] = out["batched"]["value"] / out["cpu_reference"]["value"]
+    return out
+
+
 def run_screening(args, local: int) -> dict:
     """Batched uneven screening: ligands of U[12, 64] atoms x 10 conformations x
     5 protein conformations x 8 temperatures against one 2000-point pocket, all
@@ -340,6 +406,62 @@ def run_screening(args, local: int) -> dict:
             "speedup_over_plain": batched / plain_value}
 
 
+def run_partition(args, cx, world: int, rank: int, local: int, seed: int) -> dict | None:
+    """One Complex sharded across the ranks (the product's multi-GPU path):
+    each rank runs its replica range (gd_replica_range, SetParaT's split cut at
+    protein-conformation blocks: exchange partners stay on one rank) with one
+    seed on every rank, then rank 0 gathers every final replica state over NCCL
+    (shard.gather_replicas).  Strong scaling: the complex's replicas are fixed,
+    the ranks split them.  Device time of the Monte Carlo intervals, max over
+    ranks; the gather timed separately on the host."""
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from geauxdock_b200 import dock, shard
+    from geauxdock_b200._lib import check, load
+
+    lib = load()
+    b, e = shard.replica_range(cx, world, rank)
+    h = C.c_void_p()
+    check(lib.gd_ensemble_create_complex_range(C.c_void_p(cx.ctypes.data), b, e - 1, seed, local, C.byref(h)))
+    spi = STEPS_PER_INTERVAL
+    with dock.Ensemble(h, 1) as ens:
+        ens.init()
+        ens.run(spi, spi)                 # warm-up: captures the interval graph
+        ens.sync()
+        stream = torch.cuda.ExternalStream(lib.gd_ensemble_stream(ens.h), device=torch.device("cuda", local))
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.partition_intervals):
+            ens.run(spi, spi)
+        e1.record(stream)
+        e1.synchronize()
+        ens.sync()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        reps = ens.replicas(0)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    allr = shard.gather_replicas(reps, device=f"cuda:{local}")
+    gather_ms = 1e3 * (time.perf_counter() - t0)
+    sizes = [None] * world
+    dist.all_gather_object(sizes, e - b)
+    if rank != 0:
+        return None
+    n = int(cx[0]["size"]["n_rep"])
+    assert allr is not None and len(allr) == n
+    ms = float(t.item())
+    return {"workload": "the headline complex's replicas split across the ranks (gd_replica_range), one seed",
+            "scaling": "strong", "replicas": n, "replicas_per_rank": sizes,
+            "value": n * spi * args.partition_intervals / (ms / 1e3), "unit": UNIT,
+            "ms_per_interval": ms / args.partition_intervals, "intervals": args.partition_intervals,
+            "gather": {"ms": gather_ms, "bytes": int(allr.nbytes), "how": "shard.gather_replicas, NCCL all-gather"}}
+
+
 def pe_n(job, pockets) -> int:
     return job.nlig * job.ntmp * pockets[job.pocket].nconf
 
@@ -360,7 +482,9 @@ def run_serving(args, local: int) -> dict:
     pockets = synth.serving_pockets(seed=1)
     rng = np.random.default_rng(7)
     n = args.serve_requests
-    jobs = [synth.serving_job(rng, pockets, seed=50_000 + i) for i in range(2 * n + 2)]
+    loads = [float(x) for x in args.serve_loads.split(",") if x.strip()]
+    m = args.serve_load_requests
+    jobs = [synth.serving_job(rng, pockets, seed=50_000 + i) for i in range(n + m * len(loads) + 2)]
     steps = args.serve_steps
 
     def stream(srv, batch, rate, seed):
@@ -390,9 +514,16 @@ def run_serving(args, local: int) -> dict:
         s0 = srv.stats()
         named = stream(srv, jobs[:n], args.serve_rate, 11)
         s1 = srv.stats()
-        # below capacity: 70% of the request rate the saturated run sustained
-        light_rate = 0.7 * named["req_per_s"]
-        light = stream(srv, jobs[n:n + max(8, n // 2)], light_rate, 12)
+        named["offered_over_capacity"] = args.serve_rate / named["req_per_s"]
+        # below capacity: fractions of the request rate the saturated run sustained
+        below = []
+        for k, f in enumerate(loads):
+            sa = srv.stats()
+            b = stream(srv, jobs[n + k * m:n + (k + 1) * m], f * named["req_per_s"], 12 + k)
+            sb = srv.stats()
+            b["load"] = f
+            b["gpu_busy_frac"] = (sb["device_ms"] - sa["device_ms"]) / 1e3 / b["span_s"]
+            below.append(b)
         s2 = srv.stats()
     # plain kernel, one request at a time (one launch per request per interval), a few requests
     import torch
@@ -418,16 +549,18 @@ def run_serving(args, local: int) -> dict:
              "sample": f"first 3 requests one at a time, {4 * STEPS_PER_INTERVAL} MC steps each (device time)"}
     dev_s = (s1["device_ms"] - s0["device_ms"]) / 1e3
     named["gpu_busy_frac"] = dev_s / named["span_s"]
-    light["gpu_busy_frac"] = (s2["device_ms"] - s1["device_ms"]) / 1e3 / light["span_s"]
+    named["note"] = (f"the named rate is {named['offered_over_capacity']:.1f}x the measured capacity: its queue, "
+                     "and so its latency, grow with the stream's length; these are the figures of a "
+                     f"{named['requests']}-request burst")
     return {"workload": f"Poisson arrivals, ligands log-uniform [8,80] atoms, 10x5x8 replicas, {steps} MC steps, "
                         "exchange every 50, 4 resident pockets (800/1500/2200/3000 points x 5), 100 GB HBM budget",
-            "named_rate": named, "below_capacity": light, "plain_one_launch_per_request": plain,
+            "named_rate": named, "below_capacity": below, "plain_one_launch_per_request": plain,
             "speedup_over_plain": named["value"] / plain["value"],
             "server": {"warps_per_cta": s2["warps_per_cta"], "grid": s2["grid"], "pocket_staged": s2["pocket_staged"],
                        "max_active_replicas": s2["max_active_replicas"], "rounds": s2["rounds"],
                        "launches": s2["launches"], "peak_bytes": s2["peak_bytes"]},
-            "sample": f"{named['requests']} + {light['requests']} requests (the named stream has 10000; "
-                      "bounded so the bench ends in minutes)"}
+            "sample": f"{named['requests']} + {' + '.join(str(b['requests']) for b in below)} requests (the named "
+                      "stream has 10000; bounded so the bench ends in minutes)"}
 
 
 def run_ours(args) -> None:
@@ -439,9 +572,9 @@ def run_ours(args) -> None:
 
     rank, world, local = _dist()
     torch.cuda.set_device(local)
-    if args.workload in ("screening", "serving"):
+    if args.workload in ("screening", "serving", "single"):
         if rank == 0:
-            leg = run_screening(args, local) if args.workload == "screening" else run_serving(args, local)
+            leg = {"screening": run_screening, "serving": run_serving, "single": run_single}[args.workload](args, local)
             print(json.dumps({"metric": METRIC, "workload": args.workload, **leg}))
         return
     if world > 1:
@@ -570,7 +703,9 @@ def run_ours(args) -> None:
     e2e_times = []
     check(lib.gd_set_option(b"device_base", local))   # this rank's GPU for the drop-in API
     with dock.DockSession(1, seed=77 + rank) as s:
-        s.dock(cx_h, rec_h)              # warm-up (also the first-use cost of the library)
+        s.dock(cx_h, rec_h)              # warm-up: builds the kept device state
+        cx_h[0] = cx[0]
+        s.dock(cx_h, rec_h)              # warm-up of the refill path the timed calls take
         barrier()
         for _ in range(e2e_calls):
             cx_h[0] = cx[0]              # a fresh input Complex (host setup, outside the timed call)
@@ -587,8 +722,13 @@ def run_ours(args) -> None:
         e2e_s = float(t.item())
     e2e_value = world * n_rep * e2e_steps * e2e_calls / e2e_s
 
+    # the product's multi-GPU path: one complex's replicas split across the ranks + gather
+    partition = run_partition(args, cx, world, rank, local, 1000) if world > 1 else None
+
     screening = serving = None
+    single = None
     if world == 1 and args.workload == "all":
+        single = run_single(args, local)
         screening = run_screening(args, local)
         serving = run_serving(args, local)
 
@@ -626,6 +766,10 @@ def run_ours(args) -> None:
             "clocks": ck,
             "gpu_launches": all_launches,
         }
+        if partition is not None:
+            line["partition"] = partition
+        if single is not None:
+            line["single_complex"] = single
         if screening is not None:
             line["screening"] = screening
             line["serving"] = serving

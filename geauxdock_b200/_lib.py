@@ -40,11 +40,11 @@ EXPORTED = [
     "gd_ensemble_sync", "gd_ensemble_num_replicas", "gd_ensemble_replicas", "gd_ensemble_stats",
     "gd_ensemble_autotune", "gd_ensemble_destroy", "gd_ensemble_eval_poses",
     "gd_replica_range", "gd_ensemble_create_complex_range", "gd_load_complex", "gd_ensemble_cluster",
-    "gd_ensemble_best_poses",
+    "gd_ensemble_best_poses", "gd_ensemble_snapshot_bytes", "gd_ensemble_snapshot", "gd_ensemble_restore",
     "gd_layout", "gd_optimize_enepara", "gd_ensemble_stream", "gd_fp32_peak",
     "gd_eval_poses_noalloc", "gd_noalloc_scratch_bytes",
     "gd_server_config_default", "gd_server_create", "gd_server_submit", "gd_server_poll", "gd_server_drain",
-    "gd_server_get_stats", "gd_server_destroy",
+    "gd_server_get_stats", "gd_server_destroy", "gd_server_cancel", "gd_check_report",
 ]
 
 
@@ -142,7 +142,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # GDOCK_LIB selects another build of the library (the bounds-checking
+    # libgdock_check.so in its tests)
+    p = Path(path) if path else Path(os.environ.get("GDOCK_LIB") or LIB_PATH)
     if not p.exists():
         raise GdockError(GD_E_STATE, f"{p} not built (python -m geauxdock_b200.build)")
     lib = C.CDLL(str(p))
@@ -167,6 +169,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_load_complex": (i, [vp, vp]),
         "gd_ensemble_cluster": (i, [vp, i, i, vp, C.c_float, vp, i, ip, vp, vp]),
         "gd_ensemble_best_poses": (i, [vp, i, vp, vp]),
+        "gd_ensemble_snapshot_bytes": (C.c_size_t, [vp]),
+        "gd_ensemble_snapshot": (i, [vp, vp, C.c_size_t]), "gd_ensemble_restore": (i, [vp, vp, C.c_size_t]),
         "gd_ensemble_create_complex_range": (i, [vp, i, i, C.c_uint64, i, vp]),
         "gd_optimize_enepara": (i, [vp, vp]),
         "gd_ensemble_stream": (vp, [vp]), "gd_fp32_peak": (i, [C.POINTER(C.c_double)]),
@@ -178,6 +182,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "gd_server_drain": (i, [vp, i]),
         "gd_server_get_stats": (i, [vp, vp]),
         "gd_server_destroy": (i, [vp]),
+        "gd_server_cancel": (i, [vp, ll]),
+        "gd_check_report": (i, [ip, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -19,6 +19,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgdock.so"
+# the bounds-checking build: the kernel source compiled with -DGD_CHECK (test use)
+CHECK_LIB = PKG / "libgdock_check.so"
+CHECK_SRC = "gd_mc.cu"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
               "-I", str(ROOT / "include"), "-I", str(CSRC)]
@@ -41,8 +44,8 @@ def _headers_mtime() -> float:
     return max((h.stat().st_mtime for h in hs), default=0.0)
 
 
-def _compile(src: Path, obj: Path, verbose: bool) -> None:
-    cmd = [_nvcc(), *_host_cxx(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+def _compile(src: Path, obj: Path, verbose: bool, extra: tuple = ()) -> None:
+    cmd = [_nvcc(), *_host_cxx(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -51,7 +54,8 @@ def _compile(src: Path, obj: Path, verbose: bool) -> None:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile every CUDA source for sm_100a and link libgdock.so; returns its path."""
+    """Compile every CUDA source for sm_100a and link libgdock.so (and the
+    bounds-checking libgdock_check.so); returns the product library's path."""
     BUILD.mkdir(exist_ok=True)
     srcs = sorted(CSRC.glob("*.cu"))
     hm = _headers_mtime()
@@ -62,16 +66,22 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objs.append(o)
         if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, hm):
             todo.append((s, o))
-    if todo:
-        with cf.ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 4)) as ex:
-            list(ex.map(lambda so: _compile(so[0], so[1], verbose), todo))
-    if force or todo or not LIB.exists():
-        cmd = [_nvcc(), *_host_cxx(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    chk = BUILD / (Path(CHECK_SRC).stem + "_check.o")
+    chk_src = CSRC / CHECK_SRC
+    chk_todo = force or not chk.exists() or chk.stat().st_mtime < max(chk_src.stat().st_mtime, hm)
+    jobs = [(s, o, ()) for s, o in todo] + ([(chk_src, chk, ("-DGD_CHECK",))] if chk_todo else [])
+    if jobs:
+        with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+            list(ex.map(lambda j: _compile(j[0], j[1], verbose, j[2]), jobs))
+    check_objs = [chk if o.stem == Path(CHECK_SRC).stem else o for o in objs]
+    for lib, ob, stale in ((LIB, objs, bool(todo)), (CHECK_LIB, check_objs, bool(todo) or chk_todo)):
+        if force or stale or not lib.exists():
+            cmd = [_nvcc(), *_host_cxx(), *ARCH, "-shared", "-o", str(lib), *map(str, ob)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

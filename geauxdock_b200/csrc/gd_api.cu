@@ -26,6 +26,7 @@ struct Options {
   int graph = 1;  // replay whole exchange intervals from a captured graph
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
+  int dock_device_pack = 1;  // Dock refills that state on the GPU from the Complex CopyH2D put there
   int device_base = 0;        // the drop-in API's GPU g is CUDA device device_base + g
   long long wait_limit = 0;   // microseconds of a bounded shared-memory wait (0: one second)
   int stall_test = 0;         // test hook: staging barriers that never complete (bounded waits run out)
@@ -55,6 +56,7 @@ bool same_options(const Options &a, const Options &b)
 {
   return a.kernel == b.kernel && a.precision == b.precision && a.warps == b.warps && a.kpl == b.kpl &&
          a.ab == b.ab && a.graph == b.graph && a.stage == b.stage && a.dock_cache == b.dock_cache &&
+         a.dock_device_pack == b.dock_device_pack &&
          a.device_base == b.device_base && a.wait_limit == b.wait_limit && a.stall_test == b.stall_test;
 }
 
@@ -280,8 +282,9 @@ int finish_create(gd_ensemble *e)
   }
   GD_CUDA(cudaMalloc(&e->d_step, sizeof(int)));
   GD_CUDA(cudaMalloc(&e->d_queue, sizeof(int)));
-  GD_CUDA(cudaMalloc(&e->d_err, sizeof(int)));
-  GD_CUDA(cudaMemset(e->d_err, 0, sizeof(int)));
+  // error words: [0] kernel flags (kErr*), [1..3] the device packer's failure details
+  GD_CUDA(cudaMalloc(&e->d_err, 4 * sizeof(int)));
+  GD_CUDA(cudaMemset(e->d_err, 0, 4 * sizeof(int)));
   GD_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
   const Options o = opts();
   e->kernel = o.kernel;
@@ -314,9 +317,16 @@ cudaEvent_t next_event(gd_ensemble *e)
 
 int check_err(gd_ensemble *e)
 {
-  int h = 0;
-  GD_CUDA(cudaMemcpy(&h, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (h & kErrTimeout) return fail(GD_E_TIMEOUT, "a bounded wait for a shared-memory bulk copy gave up");
+  int h[4] = {0, 0, 0, 0};
+  GD_CUDA(cudaMemcpy(h, e->d_err, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h[0] & kErrPack) {
+    if (h[1] == kPackFailShape)
+      return fail(GD_E_INVALID, "the Complex on the GPU differs in %s (%d) from the one the host described",
+                  pack_field_name(h[2]), h[3]);
+    return fail(h[1] == kPackFailCapacity ? GD_E_CAPACITY : GD_E_INVALID, "invalid Complex: %s: %d",
+                pack_field_name(h[2]), h[3]);
+  }
+  if (h[0] & kErrTimeout) return fail(GD_E_TIMEOUT, "a bounded wait for a shared-memory bulk copy gave up");
   return GD_OK;
 }
 
@@ -346,6 +356,7 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
 {
   KArgs a{};
   a.jobs = e->d_jobs;
+  a.n_jobs = (int)e->jobs.size();
   a.items = e->d_items;
   a.n_items = e->n_items;
   a.queue = e->d_queue;
@@ -489,18 +500,113 @@ int ensemble_from_complex_range(const Complex *c, int rb, int re, uint64_t seed,
   return GD_OK;
 }
 
+// The shapes Dock's cached state was packed for, read from a host Complex
+// without packing it: true if `c` (replicas [rb, re]) has exactly these.
+bool same_dock_shapes(const gd_ensemble *e, const Complex *c, int rb, int re)
+{
+  if (e->jobs.size() != 1 || e->pockets.size() != 1) return false;
+  const DevJob &J = e->jobs[0].dj;
+  const ComplexSize &sz = c->size;
+  if (sz.n_prt < 1 || sz.n_prt > GD_MAX_CONF_PRT || sz.n_lig < 1 || sz.n_lig > GD_MAX_CONF_LIG ||
+      sz.kde_npoint < 0 || sz.kde_npoint > GD_MAXKDE || sz.n_rep > GD_MAX_REP || rb < 0 || re >= sz.n_rep || rb > re)
+    return false;
+  int P = 0;
+  for (int i = 0; i < sz.n_prt; ++i) P = std::max(P, c->prt[i].prt_npoint);
+  const int Ppad = ((P + kPointAlign - 1) / kPointAlign) * kPointAlign;
+  int nk = 0;
+  for (int k = 0; k < sz.kde_npoint; ++k) nk += c->kde.t[k] >= 0 && c->kde.t[k] < kLigTypes;
+  if (J.natom != c->lig[0].lig_natom || J.nlig != sz.n_lig || J.nprt != sz.n_prt || J.ntmp != sz.n_tmp ||
+      J.nmcs != sz.mcs_nrow || J.npoint_pad != Ppad || e->pockets[0].Ppad != Ppad || J.nkde != nk ||
+      J.nrep != re - rb + 1 || J.rid_base != rb || J.nrep_total != sz.n_rep)
+    return false;
+  const std::vector<int> &prt = e->rep_prt[0];
+  for (int r = rb; r <= re; ++r)
+    if (c->replica[r].idx_prt != prt[r - rb]) return false;  // the work items group replicas by it
+  return true;
+}
+
+// Refill of Dock's cached state on the GPU: the device packer reads the
+// Complex that CopyH2D put at d_cx and writes the arenas the state already
+// holds (no host packing, no copy of packed arrays).  A Complex the packer
+// refuses sets the ensemble's error flag, which the kernels and check_err see.
+int dock_refill_device(gd_ensemble *e, const Complex *d_cx, int rb, int re, int n_rep, uint64_t seed, Record *rec)
+{
+  const DevJob &J = e->jobs[0].dj;
+  const DevPocket &pk = e->pockets[0];
+  PackDst D{};
+  D.job = e->d_jobs;
+  D.par = const_cast<DevParams *>(J.par);
+  D.ref4 = const_cast<float4 *>(J.ref4);
+  D.err = e->d_err;
+  D.lgrp = const_cast<int2 *>(J.lgrp);
+  D.lcenter = const_cast<float *>(J.lcenter);
+  D.pcenter = pk.center;
+  D.tcc = const_cast<float *>(J.tcc);
+  D.lig = const_cast<float4 *>(J.lig);
+  D.kde = const_cast<float4 *>(J.kde);
+  D.mcs = const_cast<float4 *>(J.mcs);
+  D.pos = pk.pos;
+  D.aux = pk.aux;
+  D.ncdc = pk.ncdc;
+  D.psp = const_cast<float *>(J.psp);
+  D.pspmask = const_cast<uint32_t *>(J.pspmask);
+  D.kde_cap = std::max(J.nkde, 1);
+  D.Ppad = pk.Ppad;
+  D.nkde_expect = J.nkde;
+  D.expect_L = J.natom;
+  D.expect_nlig = J.nlig;
+  D.expect_nprt = J.nprt;
+  D.expect_M = J.nmcs;
+  D.expect_ntmp = J.ntmp;
+  D.rep = J.rep;
+  D.run_acc = J.run_acc;
+  D.stats = J.stats;
+  D.minus_beta = const_cast<float *>(J.minus_beta);
+  D.rec = rec;
+  D.rep_begin = rb;
+  D.nrep = re - rb + 1;
+  D.nrep_total = n_rep;
+  D.key0 = (uint32_t)seed;
+  D.key1 = (uint32_t)(seed >> 32);
+  GD_CUDA(cudaMemsetAsync(e->d_err, 0, 4 * sizeof(int), e->st));
+  GD_CUDA(device_pack(d_cx, D, e->st));
+  e->all_launches += 3;
+  e->jobs[0].dj.key0 = D.key0;  // the host copy of the header follows the device one
+  e->jobs[0].dj.key1 = D.key1;
+  e->jobs[0].dj.rec = rec;
+  return GD_OK;
+}
+
 // Dock's ensemble on GPU `device`: the handle's cached one refilled in place
-// when the shapes are unchanged (no allocation and no reconfiguration; the
-// packed pocket is kept when the protein bytes are unchanged), else a new one,
-// which the handle then keeps.
-int dock_ensemble(gd_rng *h, const Complex *c, int rb, int re, uint64_t seed, Record *rec, int device,
-                  gd_ensemble **out)
+// when the shapes are unchanged (no allocation and no reconfiguration), by the
+// device packer from the Complex CopyH2D put on the GPU (d_cx; option
+// dock_device_pack) or else by the host packer (the packed pocket kept when
+// the protein bytes are unchanged); otherwise a new one, which the handle
+// then keeps.
+int dock_ensemble(gd_rng *h, const Complex *c, const Complex *d_cx, int rb, int re, uint64_t seed, Record *rec,
+                  int device, gd_ensemble **out)
 {
   *out = nullptr;
   const Options o = opts();
   const size_t prt_bytes = sizeof(Protein) * (size_t)std::max(0, std::min(c->size.n_prt, GD_MAX_CONF_PRT));
   gd_ensemble *e = h->dock;
   ++h->dock_calls;
+  if (e && e->device == device && same_options(h->dock_opt, o) && o.dock_device_pack && d_cx &&
+      same_dock_shapes(e, c, rb, re)) {
+    Tracer tr("refill on the GPU");
+    GD_TRY(set_device(device));
+    GD_CUDA(cudaStreamSynchronize(e->st));
+    e->step = 0;
+    e->ev_used = 0;
+    e->launches = 0;
+    e->all_launches = 0;
+    GD_TRY(dock_refill_device(e, d_cx, rb, re, c->size.n_rep, seed, rec));
+    h->dock_prt.clear();  // the host packer's record of the packed protein no longer holds
+    tr.mark("pack enqueued");
+    ++h->dock_reused;
+    *out = e;
+    return GD_OK;
+  }
   if (e && e->device == device && same_options(h->dock_opt, o) && e->jobs.size() == 1) {
     Tracer tr("refill");
     GD_TRY(set_device(device));
@@ -613,6 +719,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "dock_cache") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_cache = %lld", v);
     g_opt.dock_cache = (int)v;
+  } else if (n == "dock_device_pack") {
+    if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_device_pack = %lld", v);
+    g_opt.dock_device_pack = (int)v;
   } else if (n == "device_base") {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess) count = 0;
@@ -624,6 +733,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "stall_test") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "stall_test = %lld", v);
     g_opt.stall_test = (int)v;
+  } else if (n == "fail_alloc") {
+    if (v < 0 || v > 1000000) return fail(GD_E_INVALID, "fail_alloc = %lld", v);
+    set_injected_alloc_failures((int)v);
   } else if (n == "graph") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "graph = %lld", v);
     g_opt.graph = (int)v;
@@ -645,10 +757,12 @@ long long gd_get_option(const char *name)
   if (n == "ab") return g_opt.ab;
   if (n == "graph") return g_opt.graph;
   if (n == "stage") return g_opt.stage;
+  if (n == "dock_device_pack") return g_opt.dock_device_pack;
   if (n == "dock_cache") return g_opt.dock_cache;
   if (n == "wait_limit") return g_opt.wait_limit;
   if (n == "device_base") return g_opt.device_base;
   if (n == "stall_test") return g_opt.stall_test;
+  if (n == "fail_alloc") return injected_alloc_failures();
   return GD_E_INVALID;
 }
 
@@ -829,7 +943,7 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
     }
     // each Dock call draws a fresh stream from the handle (the reference's curand state advances)
     const uint64_t seed = rng[g]->seed + (rng[g]->calls++ << 32);
-    rc = dock_ensemble(rng[g], ch, pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], dev_of(g), &ens[g]);
+    rc = dock_ensemble(rng[g], ch, cd[g], pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], dev_of(g), &ens[g]);
   }
   tr.mark("pack+create");
   // initial energy, backend_gpu.cu:87-91: one step, no move, forced accept
@@ -958,6 +1072,7 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
   EV_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
   KArgs a{};
   a.jobs = e->d_jobs;
+  a.n_jobs = (int)e->jobs.size();
   a.items = d_items;
   a.n_items = (int)items.size();
   a.queue = e->d_queue;
@@ -1022,8 +1137,9 @@ int gd_eval_poses(const Complex *c, int n, const int *conf, const float *mm, int
     rc = upload_jobs(e);
   }
   if (rc == GD_OK && cudaMalloc(&e->d_queue, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMalloc");
-  if (rc == GD_OK && cudaMalloc(&e->d_err, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMalloc");
-  if (rc == GD_OK && cudaMemset(e->d_err, 0, sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMemset");
+  // error words as an ensemble's: kernel flags, then the device packer's details
+  if (rc == GD_OK && cudaMalloc(&e->d_err, 4 * sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMalloc");
+  if (rc == GD_OK && cudaMemset(e->d_err, 0, 4 * sizeof(int)) != cudaSuccess) rc = fail(GD_E_CUDA, "cudaMemset");
   if (rc == GD_OK && cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(GD_E_CUDA, "cudaStreamCreate");
   if (rc == GD_OK) rc = eval_on(e, 0, n, conf, mm, precision, out, out64, raw);
@@ -1343,6 +1459,106 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
     report[report_len - 1] = 0;
   }
   return rc;
+}
+
+// ---------------------------------------------------- checkpoint / resume
+namespace {
+constexpr uint64_t kSnapMagic = 0x3130504e53444723ull;  // "#GDSNP01"
+
+// Snapshot layout: SnapHeader, then per job a SnapJob, then per job its
+// ReplicaMC[nrep], int run_acc[nrep] and RepStats[nrep], in job order.
+struct SnapHeader {
+  uint64_t magic;
+  int32_t njob;
+  int32_t step;
+};
+struct SnapJob {
+  int32_t nrep, rid_base;
+  uint32_t key0, key1;
+};
+
+size_t snap_job_bytes(const DevJob &J)
+{
+  return (sizeof(ReplicaMC) + sizeof(int) + sizeof(RepStats)) * (size_t)J.nrep;
+}
+}  // namespace
+
+size_t gd_ensemble_snapshot_bytes(const gd_ensemble_t *e)
+{
+  if (!e) return 0;
+  size_t b = sizeof(SnapHeader) + sizeof(SnapJob) * e->jobs.size();
+  for (const auto &j : e->jobs) b += snap_job_bytes(j.dj);
+  return b;
+}
+
+int gd_ensemble_snapshot(gd_ensemble_t *e, void *buf, size_t bytes)
+{
+  if (!e || !buf) return fail(GD_E_INVALID, "null argument");
+  if (bytes < gd_ensemble_snapshot_bytes(e))
+    return fail(GD_E_INVALID, "snapshot buffer of %zu bytes, %zu needed", bytes, gd_ensemble_snapshot_bytes(e));
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  GD_TRY(check_err(e));
+  unsigned char *p = (unsigned char *)buf;
+  SnapHeader h{kSnapMagic, (int32_t)e->jobs.size(), (int32_t)e->step};
+  std::memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  for (const auto &j : e->jobs) {
+    const SnapJob sj{j.dj.nrep, j.dj.rid_base, j.dj.key0, j.dj.key1};
+    std::memcpy(p, &sj, sizeof sj);
+    p += sizeof sj;
+  }
+  for (const auto &j : e->jobs) {
+    const DevJob &J = j.dj;
+    GD_CUDA(cudaMemcpyAsync(p, J.rep, sizeof(ReplicaMC) * J.nrep, cudaMemcpyDeviceToHost, e->st));
+    p += sizeof(ReplicaMC) * J.nrep;
+    GD_CUDA(cudaMemcpyAsync(p, J.run_acc, sizeof(int) * J.nrep, cudaMemcpyDeviceToHost, e->st));
+    p += sizeof(int) * J.nrep;
+    GD_CUDA(cudaMemcpyAsync(p, J.stats, sizeof(RepStats) * J.nrep, cudaMemcpyDeviceToHost, e->st));
+    p += sizeof(RepStats) * J.nrep;
+  }
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  return GD_OK;
+}
+
+int gd_ensemble_restore(gd_ensemble_t *e, const void *buf, size_t bytes)
+{
+  if (!e || !buf) return fail(GD_E_INVALID, "null argument");
+  if (bytes < sizeof(SnapHeader)) return fail(GD_E_INVALID, "snapshot of %zu bytes", bytes);
+  const unsigned char *p = (const unsigned char *)buf;
+  SnapHeader h;
+  std::memcpy(&h, p, sizeof h);
+  if (h.magic != kSnapMagic) return fail(GD_E_INVALID, "not an ensemble snapshot");
+  if (h.njob != (int32_t)e->jobs.size())
+    return fail(GD_E_INVALID, "snapshot of %d jobs, ensemble has %zu", h.njob, e->jobs.size());
+  if (bytes < gd_ensemble_snapshot_bytes(e))
+    return fail(GD_E_INVALID, "snapshot of %zu bytes, this ensemble's is %zu", bytes, gd_ensemble_snapshot_bytes(e));
+  if (h.step < 0) return fail(GD_E_INVALID, "snapshot step %d", h.step);
+  p += sizeof h;
+  for (size_t k = 0; k < e->jobs.size(); ++k) {
+    SnapJob sj;
+    std::memcpy(&sj, p, sizeof sj);
+    p += sizeof sj;
+    const DevJob &J = e->jobs[k].dj;
+    // the Philox draws are keyed by (seed, replica, step): a snapshot continues
+    // bit for bit only in an ensemble of the same replicas and seeds
+    if (sj.nrep != J.nrep || sj.rid_base != J.rid_base || sj.key0 != J.key0 || sj.key1 != J.key1)
+      return fail(GD_E_INVALID, "snapshot job %zu: replicas/seed differ from the ensemble's", k);
+  }
+  GD_TRY(set_device(e->device));
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  for (const auto &j : e->jobs) {
+    const DevJob &J = j.dj;
+    GD_CUDA(cudaMemcpyAsync(J.rep, p, sizeof(ReplicaMC) * J.nrep, cudaMemcpyHostToDevice, e->st));
+    p += sizeof(ReplicaMC) * J.nrep;
+    GD_CUDA(cudaMemcpyAsync(J.run_acc, p, sizeof(int) * J.nrep, cudaMemcpyHostToDevice, e->st));
+    p += sizeof(int) * J.nrep;
+    GD_CUDA(cudaMemcpyAsync(J.stats, p, sizeof(RepStats) * J.nrep, cudaMemcpyHostToDevice, e->st));
+    p += sizeof(RepStats) * J.nrep;
+  }
+  GD_CUDA(cudaStreamSynchronize(e->st));
+  e->step = h.step;
+  return GD_OK;
 }
 
 int gd_ensemble_destroy(gd_ensemble_t *e)

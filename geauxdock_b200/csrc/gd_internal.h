@@ -179,13 +179,14 @@ enum McFlags {
 };
 
 // Error flags written by kernels into a device word.
-enum DevError { kErrNone = 0, kErrTimeout = 1, kErrSize = 2 };
+enum DevError { kErrNone = 0, kErrTimeout = 1, kErrSize = 2, kErrPack = 4 };
 
 // ---- kernels (gd_mc.cu) ----------------------------------------------------
 
 // Arguments of the batched kernel (Monte Carlo mode and pose-evaluation mode).
 struct KArgs {
   const DevJob *jobs;
+  int n_jobs;              // entries of jobs (the work items' job indices are below it)
   const WorkItem *items;
   int n_items;
   int *queue;

@@ -39,6 +39,7 @@
 
 #include "gd_device.cuh"
 #include "gd_internal.h"
+#include "gd_pack.h"
 
 namespace gd {
 
@@ -75,6 +76,31 @@ __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 }  // namespace
+
+// Bounds checks of the debug build (-DGD_CHECK, libgdock_check.so): every
+// instrumented index is compared with the length of its array; one out of
+// range records (site, index, length) in g_check once and is replaced by 0,
+// so the access stays inside the array and the run goes on.  gd_check_report
+// reads the record.  In the product build GD_AT(i, n, site) is just i.
+#ifdef GD_CHECK
+static __device__ int g_check[4];
+__device__ __forceinline__ long long check_at(long long i, long long n, int site)
+{
+  if (i >= 0 && i < n) return i;
+  if (atomicCAS(&g_check[0], 0, 1) == 0) {
+    g_check[1] = site;
+    g_check[2] = (int)i;
+    g_check[3] = (int)n;
+  }
+  return 0;
+}
+#define GD_AT(i, n, site) ::gd::check_at((long long)(i), (long long)(n), (site))
+#else
+#define GD_AT(i, n, site) (i)
+#endif
+// sites reported by gd_check_report
+enum CheckSite { kSiteLig = 1, kSiteApt, kSiteAph, kSiteAhd, kSitePos, kSitePsp, kSiteKde, kSiteMcs, kSiteLgrp,
+                 kSiteTcc, kSiteLigConf, kSitePrtConf, kSiteRep, kSiteTmp, kSiteJob, kSiteTab, kSiteTrng };
 
 // ----------------------------------------------------------- smem layout --
 struct SmemLayout {
@@ -247,7 +273,7 @@ __device__ void build_pair_tables(int L, const DevParams *par, const int2 *lg, f
   for (int e = threadIdx.x; e < npairs * kTabCols; e += blockDim.x) {
     const int i = e / kTabCols, pt = e % kTabCols;
     const int a = 2 * i, b = a + 1;
-    const int lta = lg[a].x, ltb = b < L ? lg[b].x : -1;
+    const int lta = GD_AT(lg[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab), ltb = b < L ? lg[b].x : -1;
     const float4 ta = par->tab4[lta][pt];
     const float4 tb = ltb >= 0 ? par->tab4[ltb][pt] : tab4_padding();
     apt[2 * e] = make_float4(ta.x, tb.x, ta.y, tb.y);
@@ -272,7 +298,7 @@ __device__ void build_pair_tables(int L, const DevParams *par, const int2 *lg, f
 // exactly); the charges and, for PSP, the two atom types are read from shared
 // memory where they are used, which keeps the loop within its registers.
 template <int KPL, bool HDB, bool PSP>
-__device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i, const float2 &lx,
+__device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i, int npairs, const float2 &lx,
                                                const float2 &ly, const float2 &lz, const float4 *__restrict__ apt,
                                                const float4 *__restrict__ aph, const int4 *__restrict__ ahd,
                                                const int (&pt)[KPL], const uint32_t (&pm)[KPL],
@@ -285,7 +311,7 @@ __device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, 
 #pragma unroll
   for (int j = 0; j < KPL; ++j) {
     const int e = i * kTabCols + pt[j];
-    const float4 ta = apt[2 * e], tb = apt[2 * e + 1];
+    const float4 ta = apt[2 * e], tb = apt[GD_AT(2 * e + 1, 2 * npairs * kTabCols, kSiteApt)];
     const float2 dx = __fadd2_rn(lx, npx[j]), dy = __fadd2_rn(ly, npy[j]), dz = __fadd2_rn(lz, npz[j]);
     const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
     const float2 r = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
@@ -298,19 +324,19 @@ __device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, 
     float2 g = __fmul2_rn(r, inv_el1);
     if (d2.x < c.ed2) g.x = fmaf(d2.x, fmaf(c.eb, d.x, c.ea), c.el0);
     if (d2.y < c.ed2) g.y = fmaf(d2.y, fmaf(c.eb, d.y, c.ea), c.el0);
-    acc.ele[j] = __ffma2_rn(lig[i].q, g, acc.ele[j]);
+    acc.ele[j] = __ffma2_rn(lig[GD_AT(i, npairs, kSiteLig)].q, g, acc.ele[j]);
     const float2 dmp = __fadd2_rn(d, make_float2(tb.x, tb.y));
     const float2 z = __fmul2_rn(__ffma2_rn(za, d, zb), dmp);
     const float2 e1 = __fadd2_rn(make_float2(ex2_approx(z.x), ex2_approx(z.y)), one);
     acc.pmf = __ffma2_rn(make_float2(tb.z, tb.w), make_float2(rcp_approx(e1.x), rcp_approx(e1.y)), acc.pmf);
     if constexpr (PSP) {
       const int p = row + 32 * j + lane;
-      const int lta = ahd[i].z, ltb = ahd[i].w;
-      if (((pm[j] >> lta) & 1u) && dmp.x <= 0.0f) acc.psp += __ldg(pspc + (size_t)lta * P + p);
-      if (((pm[j] >> ltb) & 1u) && dmp.y <= 0.0f) acc.psp += __ldg(pspc + (size_t)ltb * P + p);
+      const int lta = ahd[GD_AT(i, npairs, kSiteAhd)].z, ltb = ahd[i].w;
+      if (((pm[j] >> lta) & 1u) && dmp.x <= 0.0f) acc.psp += __ldg(pspc + GD_AT((size_t)lta * P + p, kLigTypes * P, kSitePsp));
+      if (((pm[j] >> ltb) & 1u) && dmp.y <= 0.0f) acc.psp += __ldg(pspc + GD_AT((size_t)ltb * P + p, kLigTypes * P, kSitePsp));
     }
     if constexpr (HDB) {
-      const float4 th = aph[e];
+      const float4 th = aph[GD_AT(e, npairs * kTabCols, kSiteAph)];
       const float2 h = __ffma2_rn(d, make_float2(th.x, th.y), make_float2(th.z, th.w));
       const float2 hh = __fmul2_rn(h, h);
       acc.hdb = __ffma2_rn(make_float2(th.x, th.y), make_float2(ex2_approx(-hh.x), ex2_approx(-hh.y)), acc.hdb);
@@ -356,9 +382,10 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     r21 = c2 * s3;
     r22 = c2 * c3;
   }
-  const float *lc = J.lcenter + 3 * ilig;
+  const float *lc = J.lcenter + 3 * GD_AT(ilig, J.nlig, kSiteLigConf);
   const T tx = (T)mm[0] + (T)lc[0], ty = (T)mm[1] + (T)lc[1], tz = (T)mm[2] + (T)lc[2];
   const float4 *lsrc = J.lig + (size_t)ilig * J.lstride;
+  const float *pc = J.pcenter + 3 * GD_AT(iprt, J.nprt, kSitePrtConf);
   for (int a = lane; a < L; a += 32) {
     const float4 v = lsrc[a];
     V4<T> o;
@@ -414,7 +441,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       uint32_t ptbits = 0u, pmbits = 0u;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
-        const int p = row + 32 * j + lane;
+        const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
         const float4 q = pos[p];
         npx[j] = f2(-q.x);
         npy[j] = f2(-q.y);
@@ -435,21 +462,21 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       for (int j = 0; j < KPL; ++j) acc.ele[j] = f2(0.0f);
       acc.psp = 0.0f;
       for (int i = 0; i < npairs; ++i) {
-        const int2 fl = *reinterpret_cast<const int2 *>(&ahd[i].x);
+        const int2 fl = *reinterpret_cast<const int2 *>(&ahd[GD_AT(i, npairs, kSiteAhd)].x);
         const bool any_hdb = ((uint32_t)fl.x & ptbits) != 0u;
         const bool any_psp = ((uint32_t)fl.y & pmbits) != 0u;
-        const float4 l01 = *reinterpret_cast<const float4 *>(&lp[i].x);
+        const float4 l01 = *reinterpret_cast<const float4 *>(&lp[GD_AT(i, npairs, kSiteLig)].x);
         const float2 lx = make_float2(l01.x, l01.y), ly = make_float2(l01.z, l01.w), lz = lp[i].z;
         if (any_hdb) {
           if (any_psp)
-            pair_atom_pair<KPL, true, true>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, true, true>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
           else
-            pair_atom_pair<KPL, true, false>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, true, false>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         } else {
           if (any_psp)
-            pair_atom_pair<KPL, false, true>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, false, true>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
           else
-            pair_atom_pair<KPL, false, false>(lp, i, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, false, false>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         }
       }
       float row_ele = 0.f;
@@ -482,7 +509,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       uint32_t ptbits = 0u, pmbits = 0u;
   #pragma unroll
       for (int j = 0; j < KPL; ++j) {
-        const int p = row + 32 * j + lane;
+        const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
         const float4 q = pos[p];
         px[j] = q.x; py[j] = q.y; pz[j] = q.z; pe[j] = q.w;
         pt[j] = __float_as_int(aux[p].y);
@@ -501,8 +528,8 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       for (int j = 0; j < KPL; ++j) acc.ele[j] = 0;
       int a = 0;
       while (a < L) {
-        const int2 grp = lgrp[a];
-        const int lt = grp.x, aend = grp.y;
+        const int2 grp = lgrp[GD_AT(a, L, kSiteLgrp)];
+        const int lt = GD_AT(grp.x, kLigTypes, kSiteTab), aend = grp.y;
         const bool any_hdb = (par->hdbmask[lt] & ptbits) != 0u;
         const bool any_psp = ((pmbits >> lt) & 1u) != 0u;
         float4 t4[KPL], rf[KPL];
@@ -525,7 +552,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         if (any_psp) {
   #pragma unroll
           for (int j = 0; j < KPL; ++j)
-            if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + (size_t)lt * P + row + 32 * j + lane);
+            if ((pm[j] >> lt) & 1u) tps[j] = __ldg(pspc + GD_AT((size_t)lt * P + row + 32 * j + lane, kLigTypes * P, kSitePsp));
         }
         if (any_hdb) {
           if (any_psp) pair_atoms<PREC, KPL, true, true>(lig, a, aend, px, py, pz, t4, t2, rf, tps, kc, acc);
@@ -577,7 +604,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           float2 npx[KPL], npy[KPL], npz[KPL], ph2[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
-            const int p = row + 32 * j + lane;
+            const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
             const float4 q = pos[p];
             npx[j] = f2(-q.x);
             npy[j] = f2(-q.y);
@@ -588,7 +615,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           for (int k = 0; k < AB / 2; ++k) {
             const int a = a0 + 2 * k;
             if (a >= L) break;
-            const LigPair la = lig[a >> 1];
+            const LigPair la = lig[GD_AT(a >> 1, (L + 1) >> 1, kSiteLig)];
 #pragma unroll
             for (int j = 0; j < KPL; ++j) {
               const float2 dx = __fadd2_rn(la.x, npx[j]), dy = __fadd2_rn(la.y, npy[j]), dz = __fadd2_rn(la.z, npz[j]);
@@ -614,7 +641,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           T px[KPL], py[KPL], pz[KPL], ph[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
-            const int p = row + 32 * j + lane;
+            const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
             const float4 q = pos[p];
             px[j] = q.x; py[j] = q.y; pz[j] = q.z;
             ph[j] = aux[p].x;
@@ -646,7 +673,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         const int a = a0 + k;
         if (a >= L) break;
         const T S = warp_sum(hpc[k]);
-        const int lt = lgrp[a].x;
+        const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
         const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
         ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
       }
@@ -678,14 +705,14 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   {
     const T kde2 = par->kde2;
     for (int a = 0; a < L;) {
-      const int2 grp = lgrp[a];
-      const int lt = grp.x, aend = grp.y;
+      const int2 grp = lgrp[GD_AT(a, L, kSiteLgrp)];
+      const int lt = GD_AT(grp.x, kLigTypes, kSiteTab), aend = grp.y;
       const int cnt = J.kcnt[lt];
       if (cnt > 0) {
         const int beg = J.kbeg[lt];
         const T inv = (T)1 / (T)cnt;
         for (int k = beg + lane; k < beg + cnt; k += 32) {
-          const float4 q = kde[k];
+          const float4 q = kde[GD_AT(k, J.nkde, kSiteKde)];
           T s = 0;
           for (int b = a; b < aend; ++b) {
             const V4<T> la = atom_at(lig, b);
@@ -715,7 +742,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       int n = 0;
       if (m < M) {
         for (int a = h; a < L; a += 2) {
-          const float4 q = J.mcs[(size_t)a * M + m];
+          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
           if (q.w != 0.0f) {
             const V4<T> la = atom_at(lig, a);
             const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
@@ -726,7 +753,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       }
       s += __shfl_xor_sync(0xffffffffu, s, 16);
       n += __shfl_xor_sync(0xffffffffu, n, 16);
-      if (m < M && h == 0) macc += (T)J.tcc[m] * sqrt(s / (T)n);
+      if (m < M && h == 0) macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
     } else
     for (int m0 = 0; m0 < M; m0 += 32) {
       const int m = m0 + lane;
@@ -734,7 +761,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         T s = 0;
         int n = 0;
         for (int a = 0; a < L; ++a) {
-          const float4 q = J.mcs[(size_t)a * M + m];
+          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
           if (q.w != 0.0f) {
             const V4<T> la = atom_at(lig, a);
             const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
@@ -742,14 +769,13 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
             ++n;
           }
         }
-        macc += (T)J.tcc[m] * sqrt(s / (T)n);
+        macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
       }
     }
   }
   const T elhm = warp_sum(macc);
 
   // ---- distance to the pocket centre, kernel_cuda_l1_montecarlo.cu:439-454
-  const float *pc = J.pcenter + 3 * iprt;
   T dst = 0;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -850,6 +876,8 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
   const SmemLayout sl = smem_layout(A.P, A.Kst, A.lig_slots, blockDim.x / 32, PREC == kFP64);
   const int warp = threadIdx.x >> 5;
   const int lane = lane_id();
+  // a Complex the device packer refused (gd_devpack.cu) leaves its job unread
+  if (*(volatile int *)A.err & kErrPack) return;
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
   uint32_t phase = 0;
@@ -861,7 +889,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     const int it = s_item;
     if (it >= A.n_items) break;
     const WorkItem wi = A.items[it];
-    const DevJob &J = A.jobs[wi.job];
+    const DevJob &J = A.jobs[GD_AT(wi.job, A.n_jobs, kSiteJob)];
     if (wi.job != prev_job || wi.prt != prev_prt) {
       if (!stage_item<PREC == kFP64>(A, J, wi, smem, sl, &bar, phase)) {
         if (threadIdx.x == 0) atomicOr(A.err, kErrTimeout);
@@ -916,7 +944,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         // ---- Monte Carlo chunk for replica r
         const int gr = J.rid_base + r;
         int *sw = reinterpret_cast<int *>(srep);
-        sw[lane] = reinterpret_cast<const int *>(J.rep + r)[lane];
+        sw[lane] = reinterpret_cast<const int *>(J.rep + GD_AT(r, J.nrep, kSiteRep))[lane];
         if (lane == 0) {
           const RepStats &S = J.stats[r];
           wst->e_sum = 0.0;
@@ -929,7 +957,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         __syncwarp();
         int acc = J.run_acc[r];
         const int ilig = srep->idx_lig, iprt = srep->idx_prt;
-        const double mbeta = (double)J.minus_beta[srep->idx_tmp];
+        const double mbeta = (double)J.minus_beta[GD_AT(srep->idx_tmp, J.ntmp, kSiteTmp)];
         Record *rec = (J.rec && (A.flags & kMcRecord)) ? J.rec + r : nullptr;
         int ne = 0;
         if (J.rec && (A.flags & kMcResetRecord)) {
@@ -1247,3 +1275,24 @@ cudaError_t launch_exchange(const DevJob *d_job, int ngroup, int ntmp, int x, cu
 }
 
 }  // namespace gd
+
+// Bounds-check record of the debug build: out4 = {1 if an index was out of
+// range, its site (gd::CheckSite), the index, the array length}; reset != 0
+// clears it.  The product build returns GD_E_STATE.
+extern "C" int gd_check_report(int *out4, int reset)
+{
+  if (!out4) return gd::fail(GD_E_INVALID, "null argument");
+#ifdef GD_CHECK
+  GD_CUDA(cudaDeviceSynchronize());
+  GD_CUDA(cudaMemcpyFromSymbol(out4, gd::g_check, 4 * sizeof(int)));
+  if (reset) {
+    const int z[4] = {0, 0, 0, 0};
+    GD_CUDA(cudaMemcpyToSymbol(gd::g_check, z, sizeof z));
+  }
+  return GD_OK;
+#else
+  (void)reset;
+  for (int i = 0; i < 4; ++i) out4[i] = 0;
+  return gd::fail(GD_E_STATE, "not a bounds-checking build (libgdock_check.so is built with -DGD_CHECK)");
+#endif
+}

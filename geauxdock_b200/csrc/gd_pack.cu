@@ -9,6 +9,7 @@
 // the reference guards with branches are folded into zeros: hdb0/hdb1 of pairs
 // with hdb0 <= 0.1 (energy_prt_v1.cu:134, hdb1 = 1/0 there) and the psp value
 // of points that are not class 2 (energy_prt_v1.cu:109).
+#include <atomic>
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -87,6 +88,21 @@ int fail(int code, const char *fmt, ...)
 }  // namespace gd
 
 extern "C" const char *gd_last_error(void) { return gd::t_err.c_str(); }
+
+namespace gd {
+namespace {
+std::atomic<int> g_fail_alloc{0};
+}
+void set_injected_alloc_failures(int n) { g_fail_alloc.store(n); }
+int injected_alloc_failures() { return g_fail_alloc.load(); }
+bool take_injected_alloc_failure()
+{
+  int n = g_fail_alloc.load();
+  while (n > 0)
+    if (g_fail_alloc.compare_exchange_weak(n, n - 1)) return true;
+  return false;
+}
+}  // namespace gd
 
 namespace gd {
 
@@ -525,12 +541,20 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   const bool alloc_rec = want_records && rec == nullptr;
   if (alloc_rec) o_rec = ar.take(sizeof(Record) * (size_t)nrep);
 
-  if (reuse && reuse->arena && reuse->bytes == ar.off && !alloc_rec) {
+  const bool reusing = reuse && reuse->arena && reuse->bytes == ar.off && !alloc_rec;
+  if (!reusing && take_injected_alloc_failure())
+    return fail(GD_E_NOMEM, "device allocation of %zu B for a job failed (injected by the fail_alloc test hook)", ar.off);
+  if (reusing) {
     out.arena = reuse->arena;
     GD_CUDA(cudaMemcpyAsync(out.arena, ar.host.data(), ar.off, cudaMemcpyHostToDevice, st));
   } else if (async) {
     // stream-ordered: no device-wide synchronisation (a pageable copy may wait for `st` only)
-    GD_CUDA(cudaMallocAsync(&out.arena, ar.off, st));
+    const cudaError_t me = cudaMallocAsync(&out.arena, ar.off, st);
+    if (me == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      return fail(GD_E_NOMEM, "cudaMallocAsync of %zu B for a job: out of device memory", ar.off);
+    }
+    GD_CUDA(me);
     if (alloc_rec) GD_CUDA(cudaMemsetAsync(out.arena, 0, ar.off, st));
     GD_CUDA(cudaMemcpyAsync(out.arena, ar.host.data(), alloc_rec ? o_rec : ar.off, cudaMemcpyHostToDevice, st));
   } else {

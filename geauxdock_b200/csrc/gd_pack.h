@@ -23,6 +23,13 @@ struct Tracer {
 // Sets the calling thread's error message; returns `code`.
 int fail(int code, const char *fmt, ...);
 
+// Test hook (option "fail_alloc"): the next n device allocations of job
+// packing report GD_E_NOMEM as a failed cudaMalloc would, without calling it.
+void set_injected_alloc_failures(int n);
+int injected_alloc_failures();
+// True (and one fewer left) if the next allocation is to fail.
+bool take_injected_alloc_failure();
+
 #define GD_CUDA(call)                                                                                \
   do {                                                                                               \
     cudaError_t e_ = (call);                                                                         \
@@ -116,6 +123,45 @@ int pack_job_async(const JobData &jd, const DevPocket &pk, const EnePara &ep, cu
 int cluster_job(const DevJob &J, const DevJob *d_job, cudaStream_t st, int ref_lig, const float ref_mm[6],
                 float rmsd_cut, gd_cluster_t *clusters, int max_clusters, int *n_clusters, int *cluster_of,
                 float *rmsd_to_ref);
+// Destination of the device-side packer (gd_devpack.cu): device arrays laid
+// out as the host packer lays them out, and the DevJob header to write.
+// err[4]: flag (kErrPack), failure kind, field id, value (zeroed by the
+// caller).  Expectations (-1 or 0: none) bound what the packer may write:
+// a Complex of other shapes fails with kPackFailShape and writes nothing past
+// the validation.
+struct PackDst {
+  DevJob *job;
+  DevParams *par;
+  float4 *ref4;
+  int *err;
+  int2 *lgrp;
+  float *lcenter, *pcenter, *tcc;
+  float4 *lig, *kde, *mcs;
+  float4 *pos;
+  float2 *aux;
+  int *ncdc;
+  float *psp;
+  uint32_t *pspmask;
+  int kde_cap;         // KDE points the kde array holds
+  int Ppad;            // > 0: padded points per conformation the arrays hold (else from the Complex)
+  int nkde_expect;     // >= 0: KDE points of ligand types the arrays hold
+  int expect_L, expect_nlig, expect_nprt, expect_M, expect_ntmp;  // >= 0: the shapes the arrays hold
+  // replicas (null rep: none): the Complex's replicas [rep_begin, rep_begin + nrep)
+  ReplicaMC *rep;
+  int *run_acc;
+  RepStats *stats;
+  float *minus_beta;
+  Record *rec;
+  int rep_begin, nrep, nrep_total;
+  uint32_t key0, key1;
+};
+enum { kPackFailCapacity = 1, kPackFailInput = 2, kPackFailShape = 3 };
+enum { kFieldNLig = 1, kFieldNPrt, kFieldNatom, kFieldNatomConf, kFieldNpoint, kFieldKde, kFieldMcs, kFieldLigType,
+       kFieldPrtType, kFieldSeq3r, kFieldMcsRow, kFieldP1a, kFieldNTmp, kFieldReplica };
+// Launches the packer on `st` (setup, pocket, ligand kernels); failures stay in D.err.
+cudaError_t device_pack(const Complex *d_cx, const PackDst &D, cudaStream_t st);
+const char *pack_field_name(int field);
+
 void free_pocket(DevPocket &p);
 void free_job(DevJobBuf &j);
 void free_job_async(DevJobBuf &j, cudaStream_t st);

@@ -39,8 +39,11 @@ __device__ __forceinline__ float block_sum(float v, float *red)
 
 }  // namespace
 
-__global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_begin, int nsteps, int flags)
+__global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_begin, int nsteps, int flags,
+                                                    const int *err)
 {
+  // a Complex the device packer refused (gd_devpack.cu) leaves its job unread
+  if (err && (*(volatile const int *)err & kErrPack)) return;
   const DevJob &J = *jobp;
   __shared__ DevParams par;
   __shared__ float4 lig_s[kMaxAtoms];
@@ -291,9 +294,8 @@ __global__ void __launch_bounds__(kBD) plain_kernel(const DevJob *jobp, int s_be
 cudaError_t launch_plain(const DevJob *d_job, int nrep, int s_begin, int nsteps, int flags, int *d_err,
                          cudaStream_t st)
 {
-  (void)d_err;
   if (nrep <= 0) return cudaSuccess;
-  plain_kernel<<<nrep, kBD, 0, st>>>(d_job, s_begin, nsteps, flags);
+  plain_kernel<<<nrep, kBD, 0, st>>>(d_job, s_begin, nsteps, flags, d_err);
   return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@
 #include <numeric>
 #include <string>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 #include "gd_internal.h"
@@ -101,6 +102,8 @@ struct gd_server {
   std::condition_variable cv_sub, cv_res, cv_idle;
   std::deque<std::unique_ptr<ServeReq>> pending;
   std::deque<gd_result_t> results;
+  std::vector<long long> cancel;   // tickets of admitted requests to cancel at the next round boundary
+  std::unordered_set<long long> live;  // tickets submitted and not yet reported
   long long next_ticket = 1;
   long long outstanding = 0;
   size_t used_bytes = 0;
@@ -145,6 +148,7 @@ void publish(gd_server *s, ServeReq &r, int status)
   res.t_admit = r.t_admit;
   res.t_done = now_s(s);
   s->results.push_back(res);
+  s->live.erase(r.ticket);
   --s->outstanding;
   if (status == GD_OK) ++s->stats.completed;
   else ++s->stats.failed;
@@ -271,6 +275,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
                           s->st));
   KArgs a{};
   a.jobs = s->d_jobs;
+  a.n_jobs = nslot;
   a.queue = s->d_queue;
   a.err = s->d_err;
   a.P = s->tc.stage ? s->Pmax : 0;
@@ -378,6 +383,31 @@ int admit(gd_server *s)
   return GD_OK;
 }
 
+// Retires the admitted requests whose cancellation was asked for: their
+// memory is freed stream-ordered after the rounds already enqueued (which
+// still name them), and they are reported as GD_E_CANCELLED.  A request whose
+// final round is already enqueued finishes normally.
+void retire_cancelled(gd_server *s)
+{
+  std::vector<long long> ask;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->cancel.empty()) return;
+    ask.swap(s->cancel);
+  }
+  for (long long t : ask)
+    for (auto &p : s->slots)
+      if (p && p->ticket == t && !p->done) {
+        free_job_async(p->buf, s->st);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->active_reps -= p->nrep;
+        release(s, *p);
+        publish(s, *p, GD_E_CANCELLED);
+        p.reset();
+        break;
+      }
+}
+
 void serve_loop(gd_server *s)
 {
   if (cudaSetDevice(s->device) != cudaSuccess) {
@@ -391,10 +421,11 @@ void serve_loop(gd_server *s)
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      auto nothing = [&] { return s->pending.empty() && s->active_reps == 0; };
+      auto nothing = [&] { return s->pending.empty() && s->active_reps == 0 && s->cancel.empty(); };
       while (!s->stop && nothing() && !prev) s->cv_sub.wait_for(lk, std::chrono::milliseconds(50));
       if (s->stop) break;
     }
+    retire_cancelled(s);
     int rc = admit(s);
     bool enq = false;
     if (rc == GD_OK) rc = enqueue_round(s, k, fin_cur, enq);
@@ -627,11 +658,29 @@ int gd_server_submit(gd_server_t *s, const gd_request_t *req, long long *ticket)
   if (s->fatal != GD_OK) return fail(s->fatal, "server stopped: %s", s->fatal_msg.c_str());
   if (s->stop) return fail(GD_E_STATE, "server is shutting down");
   r->ticket = s->next_ticket++;
+  s->live.insert(r->ticket);
   r->t_submit = now_s(s);
   if (ticket) *ticket = r->ticket;
   ++s->outstanding;
   ++s->stats.submitted;
   s->pending.push_back(std::move(r));
+  s->cv_sub.notify_all();
+  return GD_OK;
+}
+
+int gd_server_cancel(gd_server_t *s, long long ticket)
+{
+  if (!s) return fail(GD_E_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+    if ((*it)->ticket == ticket) {
+      publish(s, **it, GD_E_CANCELLED);
+      s->pending.erase(it);
+      return GD_OK;
+    }
+  if (ticket < 1 || ticket >= s->next_ticket) return fail(GD_E_INVALID, "cancel: unknown ticket %lld", ticket);
+  if (!s->live.count(ticket)) return fail(GD_E_STATE, "cancel: request %lld already finished", ticket);
+  s->cancel.push_back(ticket);
   s->cv_sub.notify_all();
   return GD_OK;
 }

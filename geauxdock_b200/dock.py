@@ -185,6 +185,18 @@ class Ensemble:
         cl = [{k: getattr(c, k) for k, _ in Cluster._fields_ if k != "pad_"} for c in out[:min(ncl.value, max_clusters)]]
         return cl, cof, rmsd
 
+    def snapshot(self) -> bytes:
+        """Checkpoint of the resident state (gd_ensemble_snapshot): replicas, accept
+        flags, FP64 statistics and the step counter."""
+        n = self.lib.gd_ensemble_snapshot_bytes(self.h)
+        buf = C.create_string_buffer(n)
+        check(self.lib.gd_ensemble_snapshot(self.h, buf, n))
+        return buf.raw
+
+    def restore(self, snap: bytes) -> None:
+        """Resume from a checkpoint of an ensemble of the same jobs and seeds."""
+        check(self.lib.gd_ensemble_restore(self.h, snap, len(snap)))
+
     def autotune(self, steps: int = 4) -> str:
         buf = C.create_string_buffer(8192)
         check(self.lib.gd_ensemble_autotune(self.h, steps, buf, len(buf)))
@@ -271,6 +283,10 @@ class Server:
 
     def drain(self, timeout_ms: int = -1) -> None:
         check(self.lib.gd_server_drain(self.h, timeout_ms))
+
+    def cancel(self, ticket: int) -> None:
+        """Cancel a queued or running request (its result reports GD_E_CANCELLED)."""
+        check(self.lib.gd_server_cancel(self.h, ticket))
 
     def stats(self) -> dict:
         from ._lib import ServerStats

@@ -108,7 +108,9 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
  * shared-memory waits last before they give up and report GD_E_TIMEOUT;
  * 0: one second), "stall_test" (test hook, 0 in normal
  * use: ensembles announce bytes to their staging barriers that no copy
- * delivers, so that the bounded waits run out).  Applies to objects created
+ * delivers, so that the bounded waits run out), "fail_alloc" (test hook, 0 in
+ * normal use: the next n device allocations for packing a job report
+ * GD_E_NOMEM without calling cudaMalloc).  Applies to objects created
  * afterwards on the calling process. */
 int gd_set_option(const char *name, long long value);
 long long gd_get_option(const char *name);
@@ -257,6 +259,18 @@ int gd_ensemble_cluster(gd_ensemble_t *e, int job, int ref_lig, const float *ref
  * of work items. */
 int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_len);
 int gd_ensemble_destroy(gd_ensemble_t *e);
+/* Checkpoint and resume of a resident ensemble: every replica's ReplicaMC,
+ * its running accept flag and FP64 statistics, and the ensemble's step
+ * counter, in one host buffer of gd_ensemble_snapshot_bytes() bytes.  The
+ * Monte Carlo and exchange draws are keyed by (seed, replica, step), so an
+ * ensemble of the same jobs and seeds restored from a snapshot continues bit
+ * for bit as the uninterrupted run would.  Restore refuses a snapshot of
+ * other replicas or seeds (GD_E_INVALID).  Both wait for the ensemble's
+ * stream.  No counterpart in the reference: it keeps the resumable state in
+ * ReplicaMC (src/common/geauxdock.h:323-336) but never saves it. */
+size_t gd_ensemble_snapshot_bytes(const gd_ensemble_t *e);
+int gd_ensemble_snapshot(gd_ensemble_t *e, void *buf, size_t bytes);
+int gd_ensemble_restore(gd_ensemble_t *e, const void *buf, size_t bytes);
 /* The CUDA stream (cudaStream_t) the ensemble launches on, for event timing. */
 void *gd_ensemble_stream(const gd_ensemble_t *e);
 
@@ -319,6 +333,13 @@ int gd_server_submit(gd_server_t *s, const gd_request_t *req, long long *ticket)
 /* Up to max finished requests; waits up to timeout_ms (-1: until one is
  * ready or nothing is outstanding).  Returns the count (>= 0). */
 int gd_server_poll(gd_server_t *s, gd_result_t *out, int max, int timeout_ms);
+/* Cancels a request: a queued one is reported at once, an admitted one at
+ * the next round boundary (its device memory freed stream-ordered behind the
+ * rounds that still use it), with status GD_E_CANCELLED.  A request whose
+ * last round is already on the GPU finishes normally instead.  GD_E_STATE if
+ * its result was already reported, GD_E_INVALID for a ticket never issued.
+ * Thread-safe. */
+int gd_server_cancel(gd_server_t *s, long long ticket);
 /* Waits until every submitted request finished (-1: no limit). */
 int gd_server_drain(gd_server_t *s, int timeout_ms);
 int gd_server_get_stats(gd_server_t *s, gd_server_stats_t *out);
@@ -348,6 +369,16 @@ typedef struct gd_load_args {
   int steps_total, steps_per_dump, steps_per_exchange;
 } gd_load_args_t;
 int gd_load_complex(const gd_load_args_t *args, Complex *out);
+
+/* Bounds checking.  libgdock_check.so is this library with its Monte Carlo /
+ * pose kernels built with -DGD_CHECK: every instrumented shared- and global-
+ * memory index is compared with its array's length, and the first one out of
+ * range is recorded (and redirected to element 0, so that the run completes
+ * without a fault).  out4 = {1 if a violation was recorded, its site, the
+ * index, the length}; reset != 0 clears the record.  Waits for the current
+ * device.  In libgdock.so it returns GD_E_STATE.  No counterpart in the
+ * reference (its IS_ASSERT toggle, src/common/toggle.h:21, is never used). */
+int gd_check_report(int *out4, int reset);
 
 /* Measured FP32 FMA throughput of the current GPU (TFLOP/s, 2 flops per FMA):
  * the denominator of the pair kernel's roofline. */

@@ -284,8 +284,11 @@ def test_dock_reuses_device_state(lib, enepara):
 
     out = {}
     try:
-        for cache in (1, 0):
+        # kept state refilled on the GPU from the device Complex, refilled by the
+        # host packer, and rebuilt on every call
+        for mode, (cache, devpack) in {"device": (1, 1), "host": (1, 0), "rebuild": (0, 1)}.items():
             check(lib.gd_set_option(b"dock_cache", cache))
+            check(lib.gd_set_option(b"dock_device_pack", devpack))
             res = []
             with dock.DockSession(1, seed=5) as s:
                 for cx in cxs:
@@ -295,11 +298,41 @@ def test_dock_reuses_device_state(lib, enepara):
                 # calls 2 and 3 keep the shapes (new ligand; new protein of the same
                 # shape) and refill the kept state; call 4 changes them
                 assert s.reuse() == (4, 2 if cache else 0)
-            out[cache] = res
+            out[mode] = res
     finally:
         check(lib.gd_set_option(b"dock_cache", 1))
-    for a, b in zip(out[1], out[0]):
-        assert a == b
+        check(lib.gd_set_option(b"dock_device_pack", 1))
+    for a, b, c in zip(out["device"], out["host"], out["rebuild"]):
+        assert a == b == c
+
+
+def test_dock_device_refill_refuses_invalid(lib, enepara):
+    """A Complex the device packer refuses on a refill (a ligand atom type out of
+    range) fails the Dock call with GD_E_INVALID before any kernel reads it; the
+    next valid call docks as a fresh session would."""
+    rng = np.random.default_rng(41)
+    pk = synth.make_pocket(rng, 300, 2)
+    temps = np.array([0.4, 1.6], np.float32)
+    cxs = [synth.to_complex(synth.make_job(rng, pk, 20, 2, 100, 5, temps, seed=s), pk, enepara, steps_total=100,
+                            steps_per_dump=50) for s in (1, 2)]
+    bad = cxs[1].copy()
+    bad[0]["lig"][0]["t2"][3] = 40
+    with dock.DockSession(1, seed=5) as s:
+        s.dock(cxs[0].copy())
+        with pytest.raises(GdockError) as ei:
+            s.dock(bad)
+        assert ei.value.code == GD_E_INVALID and "ligand atom type" in str(ei.value)
+        w = cxs[1].copy()
+        rec = s.dock(w)
+    with dock.DockSession(1, seed=5) as s2:
+        s2.dock(cxs[0].copy())
+        s2.dock(cxs[0].copy())                   # same call count: the handle's seed advances per call
+        w2 = cxs[1].copy()
+        rec2 = s2.dock(w2)
+    n = int(cxs[1][0]["size"]["n_rep"])
+    for f in w[0]["replica"].dtype.names:
+        assert w[0]["replica"][f][:n].tobytes() == w2[0]["replica"][f][:n].tobytes(), f
+    assert rec["next_entry"][:n].tobytes() == rec2["next_entry"][:n].tobytes()
 
 
 def test_sharded_run_equals_single(lib, enepara):
@@ -421,3 +454,44 @@ def test_empty_inputs(lib, enepara, oracle_lib):
         want, _ = oracle_lib.energy(cx, int(got[r]["idx_lig"]), int(got[r]["idx_prt"]), cx[0]["replica"][r]["movematrix"])
         _close(got[r]["energy"], want)
         assert int(rec[r]["next_entry"]) == 0
+
+
+def test_snapshot_restore_bit_identical(lib, enepara):
+    """Checkpoint / resume: run(100) + snapshot, then restore into a fresh
+    ensemble of the same jobs and seeds and run(100) more -- replicas and FP64
+    statistics are bit-identical to an uninterrupted run(200) (exchange every
+    20 steps, so the sweep index comes from the restored step counter)."""
+    cx = _small_ensemble(enepara, seed=21)
+    with dock.Ensemble.from_complexes([cx], [9]) as ens:
+        ens.init()
+        ens.run(200, 20)
+        ens.sync()
+        want, want_st = ens.replicas(0), ens.stats(0)
+    with dock.Ensemble.from_complexes([cx], [9]) as ens:
+        ens.init()
+        ens.run(100, 20)
+        ens.sync()
+        snap = ens.snapshot()
+        ens.run(60, 20)                          # diverges from the snapshot
+        ens.sync()
+    with dock.Ensemble.from_complexes([cx], [9]) as ens:
+        ens.restore(snap)
+        ens.run(100, 20)
+        ens.sync()
+        got, got_st = ens.replicas(0), ens.stats(0)
+    for f in want.dtype.names:
+        assert got[f].tobytes() == want[f].tobytes(), f
+    assert got_st.tobytes() == want_st.tobytes()
+
+
+def test_restore_refuses_other_seed(lib, enepara):
+    cx = _small_ensemble(enepara, seed=22)
+    with dock.Ensemble.from_complexes([cx], [1]) as a, dock.Ensemble.from_complexes([cx], [2]) as b:
+        a.init()
+        a.sync()
+        snap = a.snapshot()
+        with pytest.raises(GdockError) as ei:
+            b.restore(snap)
+        assert ei.value.code == GD_E_INVALID
+        with pytest.raises(GdockError):
+            b.restore(b"not a snapshot" * 4)

@@ -115,3 +115,69 @@ def test_bad_requests_refused(lib, enepara):
         srv.drain(60_000)
         (r,) = srv.poll(4, 0)
         assert r["ticket"] == t and r["status"] == 0
+
+
+def test_cancel_queued_and_running(lib, enepara):
+    """gd_server_cancel: a queued request is reported at once, a running one at
+    the next round boundary, both with GD_E_CANCELLED; the server keeps serving
+    and a later request's result equals its ensemble result."""
+    from geauxdock_b200._lib import GD_E_CANCELLED, GD_E_STATE
+
+    pockets = _pockets()
+    jobs = _jobs(pockets, 3)
+    # jobs 0 and 2 have 16 replicas (pocket 0), job 1 has 24 (pocket 1): with a
+    # cap of 24 replicas per round the second request waits while the first runs
+    with dock.Server(pockets, enepara, max_active_replicas=24) as srv:
+        t_run = srv.submit(jobs[0], 200_000, 50)
+        t_queued = srv.submit(jobs[2], 50, 50)
+        srv.cancel(t_queued)
+        t0 = time.time()
+        while srv.stats()["rounds"] < 3 and time.time() - t0 < 60:
+            time.sleep(0.01)
+        srv.cancel(t_run)
+        srv.drain(60_000)
+        res = {r["ticket"]: r for r in srv.poll(8, 0)}
+        assert res[t_queued]["status"] == GD_E_CANCELLED and res[t_queued]["steps"] == 0
+        assert res[t_run]["status"] == GD_E_CANCELLED and 0 < res[t_run]["steps"] < 200_000
+        with pytest.raises(GdockError) as ei:
+            srv.cancel(t_run)                    # already reported
+        assert ei.value.code == GD_E_STATE
+        with pytest.raises(GdockError) as ei:
+            srv.cancel(10_000)                   # never issued
+        assert ei.value.code == GD_E_INVALID
+        t_ok = srv.submit(jobs[1], 75, 30)
+        srv.drain(60_000)
+        (r,) = srv.poll(4, 0)
+        st = srv.stats()
+    assert r["ticket"] == t_ok and r["status"] == 0
+    want, want_st = _ensemble_result(pockets, jobs[1], enepara, 75, 30)
+    for f in want.dtype.names:
+        assert r["replicas"][f].tobytes() == want[f].tobytes(), f
+    assert st["completed"] == 1 and st["failed"] == 2 and st["outstanding"] == 0
+
+
+def test_injected_allocation_failure(lib, enepara):
+    """An allocation failure while admitting a request (injected on the host by
+    the fail_alloc hook, as a failed cudaMalloc reports it) fails that request
+    with GD_E_NOMEM; the other requests and the server carry on."""
+    from geauxdock_b200._lib import GD_E_NOMEM, check
+
+    pockets = _pockets()
+    jobs = _jobs(pockets, 3)
+    with dock.Server(pockets, enepara) as srv:
+        check(lib.gd_set_option(b"fail_alloc", 1))
+        try:
+            t1 = srv.submit(jobs[0], 50, 50)
+            srv.drain(60_000)
+        finally:
+            left = lib.gd_get_option(b"fail_alloc")
+            check(lib.gd_set_option(b"fail_alloc", 0))
+        assert left == 0
+        t2 = srv.submit(jobs[1], 50, 50)
+        t3 = srv.submit(jobs[2], 40, 20)
+        srv.drain(60_000)
+        res = {r["ticket"]: r for r in srv.poll(8, 0)}
+        st = srv.stats()
+    assert res[t1]["status"] == GD_E_NOMEM
+    assert res[t2]["status"] == 0 and res[t3]["status"] == 0
+    assert st["failed"] == 1 and st["completed"] == 2 and st["used_bytes"] == 0

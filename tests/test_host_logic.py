@@ -81,6 +81,13 @@ def test_options_validated(lib):
         check(lib.gd_set_option(b"stage", 2))
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"graph", 2))
+    # the allocation-failure test hook counts down and is off by default
+    assert lib.gd_get_option(b"fail_alloc") == 0
+    check(lib.gd_set_option(b"fail_alloc", 2))
+    assert lib.gd_get_option(b"fail_alloc") == 2
+    check(lib.gd_set_option(b"fail_alloc", 0))
+    with pytest.raises(GdockError):
+        check(lib.gd_set_option(b"fail_alloc", -1))
 
 
 def test_eval_rejects_bad_conformation_before_device_work(lib, enepara):
