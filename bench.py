@@ -102,6 +102,8 @@ def _args():
     p.add_argument("--serve-max-active", type=int, default=0,
                    help="replicas per serving round (0: the server's default, four waves of resident replicas)")
     p.add_argument("--serve-round", type=int, default=STEPS_PER_INTERVAL, help="MC steps per serving round")
+    p.add_argument("--serve-replica-warps", type=int, default=1,
+                   help="warps per replica in the server (2, 4, 8: latency mode)")
     p.add_argument("--partition-intervals", type=int, default=5,
                    help="exchange intervals timed in the multi-GPU partition leg (one complex split across ranks)")
     return p.parse_args()
@@ -306,8 +308,11 @@ def run_single(args, local: int) -> dict:
     cx = synth.to_complex(job, pk, ep, steps_total=args.single_steps, steps_per_dump=200)
     out = {"workload": "1 complex: ligand 24 atoms, pocket 600 points, 200 KDE points, 8 MCS templates, "
                        f"1 temperature, 1 replica, {args.single_steps} MC steps"}
-    for name, kern in (("batched", 0), ("plain", 1)):
+    # batched kernel with the replica on 1, 2, 4, 8 warps (latency mode), and the plain kernel
+    for name, kern, g in (("batched", 0, 1), ("batched_2_warps", 0, 2), ("batched_4_warps", 0, 4),
+                          ("batched_8_warps", 0, 8), ("plain", 1, 1)):
         check(lib.gd_set_option(b"kernel", kern))
+        check(lib.gd_set_option(b"replica_warps", g))
         try:
             with dock.Ensemble.from_complexes([cx], [1]) as ens:
                 ens.init()
@@ -323,6 +328,7 @@ def run_single(args, local: int) -> dict:
                 ms = a.elapsed_time(b)
         finally:
             check(lib.gd_set_option(b"kernel", 0))
+            check(lib.gd_set_option(b"replica_warps", 1))
         out[name] = {"value": args.single_steps / (ms / 1e3), "unit": UNIT, "ms": ms}
     from oracle import oracle as O
 
@@ -340,6 +346,7 @@ def run_single(args, local: int) -> dict:
         out["cpu_reference"] = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "reference",
                                 "sample": f"{n} of the {args.single_steps} MC steps, reference MonteCarlo_d"}
         out["speedup_batched_over_cpu"] = out["batched"]["value"] / out["cpu_reference"]["value"]
+        out["speedup_batched_8_warps_over_cpu"] = out["batched_8_warps"]["value"] / out["cpu_reference"]["value"]
     return out
 
 
@@ -506,7 +513,7 @@ def run_serving(args, local: int) -> dict:
                 "value": evals / span, "unit": UNIT, "req_per_s": len(batch) / span, "span_s": span}
 
     with dock.Server(pockets, ep, device=local, max_atoms=80, max_active_replicas=args.serve_max_active,
-                     steps_per_round=args.serve_round) as srv:
+                     steps_per_round=args.serve_round, replica_warps=args.serve_replica_warps) as srv:
         srv.submit(jobs[-1], 100, STEPS_PER_INTERVAL, results=False)   # warm-up
         srv.submit(jobs[-2], 100, STEPS_PER_INTERVAL, results=False)
         srv.drain(900_000)

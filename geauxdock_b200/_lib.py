@@ -53,7 +53,7 @@ class ServerConfig(C.Structure):
     _fields_ = [
         ("hbm_budget_bytes", C.c_ulonglong), ("max_active_replicas", C.c_int), ("max_jobs", C.c_int),
         ("max_replicas_per_job", C.c_int), ("max_atoms", C.c_int), ("steps_per_round", C.c_int),
-        ("kde_stage", C.c_int), ("warps", C.c_int), ("device", C.c_int),
+        ("kde_stage", C.c_int), ("warps", C.c_int), ("device", C.c_int), ("replica_warps", C.c_int),
     ]
 
 

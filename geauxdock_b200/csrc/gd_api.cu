@@ -27,6 +27,7 @@ struct Options {
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
   int dock_device_pack = 1;  // Dock refills that state on the GPU from the Complex CopyH2D put there
+  int replica_warps = 1;     // warps per replica (1, 2, 4, 8): latency mode of the batched FP32 kernel
   int device_base = 0;        // the drop-in API's GPU g is CUDA device device_base + g
   long long wait_limit = 0;   // microseconds of a bounded shared-memory wait (0: one second)
   int stall_test = 0;         // test hook: staging barriers that never complete (bounded waits run out)
@@ -56,7 +57,7 @@ bool same_options(const Options &a, const Options &b)
 {
   return a.kernel == b.kernel && a.precision == b.precision && a.warps == b.warps && a.kpl == b.kpl &&
          a.ab == b.ab && a.graph == b.graph && a.stage == b.stage && a.dock_cache == b.dock_cache &&
-         a.dock_device_pack == b.dock_device_pack &&
+         a.dock_device_pack == b.dock_device_pack && a.replica_warps == b.replica_warps &&
          a.device_base == b.device_base && a.wait_limit == b.wait_limit && a.stall_test == b.stall_test;
 }
 
@@ -127,7 +128,7 @@ int build_items(gd_ensemble *e)
 {
   std::vector<WorkItem> items;
   std::vector<double> cost;
-  const int R = e->tc.warps_per_cta;
+  const int R = e->tc.warps_per_cta / std::max(1, e->tc.group);  // replicas per CTA
   for (int j = 0; j < (int)e->jobs.size(); ++j) {
     const std::vector<int> &pr = e->rep_prt[j];
     const double c = (double)e->jobs[j].dj.natom * e->jobs[j].dj.npoint_pad;
@@ -157,23 +158,28 @@ int build_items(gd_ensemble *e)
   return GD_OK;
 }
 
-size_t smem_for(const gd_ensemble *e, int warps, int kst, int stage = 1)
+size_t smem_for(const gd_ensemble *e, int warps, int kst, int stage = 1, int group = 1)
 {
-  return kernel_smem_bytes(stage ? e->Pmax : 0, kst, e->lig_slots, warps, e->precision);
+  return kernel_smem_bytes(stage ? e->Pmax : 0, kst, e->lig_slots, warps, e->precision, group);
 }
 
 // Pick the KDE staging, the grid and (if not given) the replicas per CTA.
 int configure(gd_ensemble *e, TileConfig tc)
 {
-  if (tc.warps_per_cta < 1 || tc.warps_per_cta * 32 > kMaxCtaThreads)
-    return fail(GD_E_INVALID, "replicas per CTA = %d outside [1, %d]", tc.warps_per_cta, kMaxCtaThreads / 32);
+  // the split (latency) form exists for the FP32 atom-pair loop of the batched kernel
+  if (e->precision == GD_PREC_FP64 || e->kernel == GD_KERNEL_PLAIN || tc.kpl % 2) tc.group = 1;
+  if (tc.group != 1 && tc.group != 2 && tc.group != 4 && tc.group != 8)
+    return fail(GD_E_INVALID, "warps per replica = %d (1, 2, 4 or 8)", tc.group);
+  if (tc.warps_per_cta < 1 || tc.warps_per_cta * 32 > kMaxCtaThreads || tc.warps_per_cta % tc.group)
+    return fail(GD_E_INVALID, "warps per CTA = %d outside [1, %d] or not a multiple of the %d warps per replica",
+                tc.warps_per_cta, kMaxCtaThreads / 32, tc.group);
   // a pocket too large to stage is read through L1; KDE points that do not fit are read from global memory
-  if (tc.stage && smem_for(e, tc.warps_per_cta, 0, 1) > kSmemLimit) tc.stage = 0;
+  if (tc.stage && smem_for(e, tc.warps_per_cta, 0, 1, tc.group) > kSmemLimit) tc.stage = 0;
   // FP32 reads the KDE points through L1 (the shared memory left to L1 pays more than
   // staging them); FP64 stages them
   e->Kst = e->precision == GD_PREC_FP64 ? e->Kmax : 0;
-  if (smem_for(e, tc.warps_per_cta, e->Kst, tc.stage) > kSmemLimit) e->Kst = 0;
-  const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst, tc.stage);
+  if (smem_for(e, tc.warps_per_cta, e->Kst, tc.stage, tc.group) > kSmemLimit) e->Kst = 0;
+  const size_t smem = smem_for(e, tc.warps_per_cta, e->Kst, tc.stage, tc.group);
   if (smem > kSmemLimit)
     return fail(GD_E_CAPACITY, "%d replicas per CTA need %zu B of shared memory (limit %zu)", tc.warps_per_cta, smem,
                 kSmemLimit);
@@ -200,16 +206,20 @@ int choose_warps(gd_ensemble *e, TileConfig base, int stage_opt = -1)
   int nsm = 0;
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
   double best = 1e300;
-  int best_w = 8, best_stage = 1;
+  const int G = (e->precision == GD_PREC_FP64 || e->kernel == GD_KERNEL_PLAIN || base.kpl % 2) ? 1
+                                                                                         : std::max(1, base.group);
+  int best_w = std::max(8, G), best_stage = 1;
   for (int stage = 1; stage >= 0; --stage)
-  for (int w = 2; w <= kMaxCtaThreads / 32; ++w) {
+  for (int w = std::max(2, G); w <= kMaxCtaThreads / 32; w += (w < G ? 1 : G)) {
     if (stage_opt >= 0 && stage != stage_opt) continue;
+    if (w % G) continue;
     TileConfig tc = base;
     tc.warps_per_cta = w;
     tc.stage = stage;
+    tc.group = G;
     int kst = e->Kmax;
-    if (smem_for(e, w, kst, stage) > kSmemLimit) kst = 0;
-    const size_t smem = smem_for(e, w, kst, stage);
+    if (smem_for(e, w, kst, stage, G) > kSmemLimit) kst = 0;
+    const size_t smem = smem_for(e, w, kst, stage, G);
     if (smem > kSmemLimit) continue;
     const int occ = kernel_occupancy(0, e->precision, tc, smem);
     if (occ < 1) continue;
@@ -220,7 +230,7 @@ int choose_warps(gd_ensemble *e, TileConfig base, int stage_opt = -1)
       int r = 0;
       while (r < (int)pr.size()) {
         int k = 1;
-        while (r + k < (int)pr.size() && k < w && pr[r + k] == pr[r]) ++k;
+        while (r + k < (int)pr.size() && k < w / G && pr[r + k] == pr[r]) ++k;
         ++items;
         r += k;
       }
@@ -240,6 +250,7 @@ int choose_warps(gd_ensemble *e, TileConfig base, int stage_opt = -1)
   TileConfig tc = base;
   tc.warps_per_cta = best_w;
   tc.stage = best_stage;
+  tc.group = G;
   return configure(e, tc);
 }
 
@@ -292,8 +303,8 @@ int finish_create(gd_ensemble *e)
   e->use_graph = o.graph != 0;
   e->wait_limit = (uint32_t)o.wait_limit;
   e->stall_bytes = o.stall_test ? 16u : 0u;
-  TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab, o.stage != 0 ? 1 : 0};
-  if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
+  TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab, o.stage != 0 ? 1 : 0, o.replica_warps};
+  if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8, tc.group = 1;
   if (o.warps > 0) return configure(e, tc);
   return choose_warps(e, tc, o.stage);
 }
@@ -368,6 +379,7 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
   a.P = e->tc.stage ? e->Pmax : 0;
   a.Kst = e->Kst;
   a.lig_slots = e->lig_slots;
+  a.group = e->tc.group;
   a.wait_limit = e->wait_limit;
   a.stall_bytes = e->stall_bytes;
   return a;
@@ -719,6 +731,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "dock_cache") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_cache = %lld", v);
     g_opt.dock_cache = (int)v;
+  } else if (n == "replica_warps") {
+    if (v != 1 && v != 2 && v != 4 && v != 8) return fail(GD_E_INVALID, "replica_warps = %lld (1, 2, 4 or 8)", v);
+    g_opt.replica_warps = (int)v;
   } else if (n == "dock_device_pack") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_device_pack = %lld", v);
     g_opt.dock_device_pack = (int)v;
@@ -757,6 +772,7 @@ long long gd_get_option(const char *name)
   if (n == "ab") return g_opt.ab;
   if (n == "graph") return g_opt.graph;
   if (n == "stage") return g_opt.stage;
+  if (n == "replica_warps") return g_opt.replica_warps;
   if (n == "dock_device_pack") return g_opt.dock_device_pack;
   if (n == "dock_cache") return g_opt.dock_cache;
   if (n == "wait_limit") return g_opt.wait_limit;
@@ -1392,7 +1408,7 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   double best_t = 1e300;
   const int shapes[][2] = {{1, 8}, {2, 4}, {2, 8}, {4, 4}};
   const int warps[] = {4, 6, 8, 10, 12, 14, 16};
-  const bool can_stage = smem_for(e, 4, 0, 1) <= kSmemLimit;
+  const bool can_stage = smem_for(e, std::max(4, e->tc.group), 0, 1, e->tc.group) <= kSmemLimit;
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
@@ -1404,7 +1420,9 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
     if (e->precision != GD_PREC_FP64 && sh[0] == 1) continue;
     for (int w : warps) {
       if (rc != GD_OK) break;
-      TileConfig tc{w, sh[0], sh[1], stage};
+      // the warps per replica are kept; the candidates are the multiples of it
+      if (w % e->tc.group) continue;
+      TileConfig tc{w, sh[0], sh[1], stage, e->tc.group};
       if (configure(e, tc) != GD_OK || e->tc.stage != stage) continue;
       // a strided sample of the work items (heaviest-first order kept), about two
       // waves of the grid, so that a candidate runs the full chunk length

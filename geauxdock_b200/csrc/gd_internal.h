@@ -166,6 +166,8 @@ struct TileConfig {
   int kpl;             // pocket points per lane per row (1, 2 or 4)
   int ab;              // ligand atoms per register block (4 or 8)
   int stage = 1;       // 1: stage the protein conformation in shared memory, 0: read it through L1
+  int group = 1;       // warps per replica (1, 2, 4 or 8; FP32 only): a replica's pair rows, KDE points and
+                       // hydrophobic sums split over them (latency mode)
 };
 
 enum Precision { kFP32 = 0, kFP32Kahan = 1, kFP64 = 2 };
@@ -186,7 +188,6 @@ enum DevError { kErrNone = 0, kErrTimeout = 1, kErrSize = 2, kErrPack = 4 };
 // Arguments of the batched kernel (Monte Carlo mode and pose-evaluation mode).
 struct KArgs {
   const DevJob *jobs;
-  int n_jobs;              // entries of jobs (the work items' job indices are below it)
   const WorkItem *items;
   int n_items;
   int *queue;
@@ -203,11 +204,14 @@ struct KArgs {
   float *out;
   double *out64;
   float *raw;
+  // (after the fields above, whose offsets the kernels' register allocation turned out to depend on)
+  int n_jobs;              // entries of jobs (the work items' job indices are below it)
+  int group;               // warps per replica (TileConfig::group); 0 reads as 1
 };
 
 // Shared-memory bytes of the batched kernel for pocket conformations of P
 // points, Kst KDE points staged, lig_slots ligand atoms and `warps` replicas per CTA.
-size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision);
+size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision, int group = 1);
 
 // Resident CTAs per SM of the batched kernel for this configuration (0 if it cannot launch).
 int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem);

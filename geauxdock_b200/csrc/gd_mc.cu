@@ -81,7 +81,7 @@ __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 // instrumented index is compared with the length of its array; one out of
 // range records (site, index, length) in g_check once and is replaced by 0,
 // so the access stays inside the array and the run goes on.  gd_check_report
-// reads the record.  In the product build GD_AT(i, n, site) is just i.
+// reads the record.  In the product build GD_AT(i, n, site) is the tokens of i.
 #ifdef GD_CHECK
 static __device__ int g_check[4];
 __device__ __forceinline__ long long check_at(long long i, long long n, int site)
@@ -95,8 +95,13 @@ __device__ __forceinline__ long long check_at(long long i, long long n, int site
   return 0;
 }
 #define GD_AT(i, n, site) ::gd::check_at((long long)(i), (long long)(n), (site))
+#define GD_CHECK_ARG(...) , __VA_ARGS__
 #else
-#define GD_AT(i, n, site) (i)
+// unparenthesised on purpose: the index expression keeps its own grouping
+// (a pointer plus an index sum is then computed as written), so that the
+// product build compiles to exactly the code without the checks
+#define GD_AT(i, n, site) i
+#define GD_CHECK_ARG(...)
 #endif
 // sites reported by gd_check_report
 enum CheckSite { kSiteLig = 1, kSiteApt, kSiteAph, kSiteAhd, kSitePos, kSitePsp, kSiteKde, kSiteMcs, kSiteLgrp,
@@ -104,12 +109,18 @@ enum CheckSite { kSiteLig = 1, kSiteApt, kSiteAph, kSiteAhd, kSitePos, kSitePsp,
 
 // ----------------------------------------------------------- smem layout --
 struct SmemLayout {
-  uint32_t params, lgrp, pos, aux, kde, apt, aph, ahd, warp0, warp_bytes, lig_bytes, total;
+  uint32_t params, lgrp, pos, aux, kde, apt, aph, ahd, warp0, warp_bytes, lig_bytes, parts, total;
 };
+
+// Per-warp partial sums of a replica split over several warps (latency mode):
+// the dense terms, then the hydrophobic sum of every atom.
+constexpr int kPartTerms = 8;    // vdw, ele, pmf, psp, hdb, kde, (2 unused)
+constexpr uint32_t kPartBytes = 4u * (kPartTerms + kMaxAtoms);
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
-__host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots, int warps, bool fp64)
+__host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots, int warps, bool fp64,
+                                                   int group = 1)
 {
   SmemLayout s;
   uint32_t off = 0;
@@ -132,13 +143,40 @@ __host__ __device__ inline SmemLayout smem_layout(int P, int Kst, int lig_slots,
   s.ahd = off;
   off = align16(off + 16u * npairs);
   s.lig_bytes = (uint32_t)lig_slots * (fp64 ? 32u : 16u);  // V4<double> per atom, or LigPair per two atoms
-  // per warp: rotated ligand, ReplicaMC state, EnergyScratch (192 B), WarpStats (64 B)
-  s.warp_bytes = align16(s.lig_bytes + (uint32_t)sizeof(ReplicaMC) + 192u + 64u);
+  // per warp: rotated ligand, ReplicaMC state, EnergyScratch (192 B), WarpStats (64 B), and with
+  // several warps per replica its partial sums
+  s.parts = s.lig_bytes + (uint32_t)sizeof(ReplicaMC) + 192u + 64u;
+  s.warp_bytes = align16(s.parts + (group > 1 ? kPartBytes : 0u));
   s.warp0 = off;
   off += s.warp_bytes * (uint32_t)warps;
   s.total = off;
   return s;
 }
+
+// warps per replica a launch runs with: pose evaluation and FP64 use one
+template <int MODE, int PREC>
+__host__ __device__ inline int kernel_group(const KArgs &a)
+{
+  return (MODE == 1 || PREC == kFP64 || a.group < 1) ? 1 : a.group;
+}
+
+// Barrier of the G warps of one replica (named barrier 1 + index of the group).
+__device__ __forceinline__ void group_sync(int bar_id, int G)
+{
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(G * 32) : "memory");
+}
+
+// A replica's place in a group of G warps (latency mode): warp `sub` of the
+// group takes pair rows sub, sub + G, ... and KDE points likewise; its partial
+// sums go to its own part area (gparts + sub * pstride floats) and warp 0 of
+// the group combines them in warp order, so that the result depends on G but
+// on nothing else.  G = 1 is the plain one-warp-per-replica evaluation.
+struct Split {
+  int sub, G, bar_id;
+  float *gparts;
+  uint32_t pstride;
+};
+struct NoSplit {};  // the one-warp-per-replica instantiation takes no split argument
 
 // ------------------------------------------------------------- energy --
 // Energy of ligand conformation ilig at pose mm in protein conformation iprt.
@@ -298,7 +336,7 @@ __device__ void build_pair_tables(int L, const DevParams *par, const int2 *lg, f
 // exactly); the charges and, for PSP, the two atom types are read from shared
 // memory where they are used, which keeps the loop within its registers.
 template <int KPL, bool HDB, bool PSP>
-__device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i, int npairs, const float2 &lx,
+__device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i GD_CHECK_ARG(int npairs), const float2 &lx,
                                                const float2 &ly, const float2 &lz, const float4 *__restrict__ apt,
                                                const float4 *__restrict__ aph, const int4 *__restrict__ ahd,
                                                const int (&pt)[KPL], const uint32_t (&pm)[KPL],
@@ -344,15 +382,23 @@ __device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, 
   }
 }
 
-template <int PREC, int KPL, int AB>
+template <int PREC, int KPL, int AB, bool SPLIT = false>
 __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__restrict__ par,
                                          const float4 *__restrict__ pos, const float2 *__restrict__ aux,
                                          const float4 *__restrict__ kde, const int2 *__restrict__ lgrp,
                                          const float4 *__restrict__ apt, const float4 *__restrict__ aph,
                                          const int4 *__restrict__ ahd, void *ligbuf, int ilig, int iprt,
-                                         const float *mm, EnergyScratch *out)
+                                         const float *mm, EnergyScratch *out,
+                                         typename std::conditional<SPLIT, Split, NoSplit>::type sp = {})
 {
   using T = typename std::conditional<PREC == kFP64, double, float>::type;
+  // SPLIT: the latency-mode instantiation (G warps per replica); otherwise G is 1 at compile time
+  int G = 1, my_sub = 0;
+  if constexpr (SPLIT && PREC != kFP64) {
+    G = sp.G;
+    my_sub = sp.sub;
+  }
+  const int row0 = 32 * KPL * my_sub, rstep = 32 * KPL * G;
   const int lane = lane_id();
   const int L = J.natom;
   const int P = J.npoint_pad;
@@ -385,7 +431,6 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   const float *lc = J.lcenter + 3 * GD_AT(ilig, J.nlig, kSiteLigConf);
   const T tx = (T)mm[0] + (T)lc[0], ty = (T)mm[1] + (T)lc[1], tz = (T)mm[2] + (T)lc[2];
   const float4 *lsrc = J.lig + (size_t)ilig * J.lstride;
-  const float *pc = J.pcenter + 3 * GD_AT(iprt, J.nprt, kSitePrtConf);
   for (int a = lane; a < L; a += 32) {
     const float4 v = lsrc[a];
     V4<T> o;
@@ -434,7 +479,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     // table entries come per atom pair, so there is no loop over type groups
     const LigPair *lp = lig;
     const int npairs = (L + 1) >> 1;
-    for (int row = 0; row < P; row += 32 * KPL) {
+    for (int row = row0; row < P; row += rstep) {
       float2 npx[KPL], npy[KPL], npz[KPL];
       int pt[KPL];
       uint32_t pm[KPL];
@@ -469,14 +514,14 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         const float2 lx = make_float2(l01.x, l01.y), ly = make_float2(l01.z, l01.w), lz = lp[i].z;
         if (any_hdb) {
           if (any_psp)
-            pair_atom_pair<KPL, true, true>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, true, true>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
           else
-            pair_atom_pair<KPL, true, false>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, true, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         } else {
           if (any_psp)
-            pair_atom_pair<KPL, false, true>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, false, true>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
           else
-            pair_atom_pair<KPL, false, false>(lp, i, npairs, lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+            pair_atom_pair<KPL, false, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
         }
       }
       float row_ele = 0.f;
@@ -502,7 +547,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       }
     }
   } else {
-    for (int row = 0; row < P; row += 32 * KPL) {
+    for (int row = row0; row < P; row += rstep) {
       T px[KPL], py[KPL], pz[KPL], pe[KPL];
       int pt[KPL];
       uint32_t pm[KPL];
@@ -600,7 +645,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         float2 h2[AB / 2];
 #pragma unroll
         for (int k = 0; k < AB / 2; ++k) h2[k] = f2(0.0f);
-        for (int row = 0; row < rows; row += 32 * KPL) {
+        for (int row = row0; row < rows; row += rstep) {
           float2 npx[KPL], npy[KPL], npz[KPL], ph2[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
@@ -637,7 +682,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       } else {
 #pragma unroll
         for (int k = 0; k < AB; ++k) hpc[k] = 0;
-        for (int row = 0; row < rows; row += 32 * KPL) {
+        for (int row = row0; row < rows; row += rstep) {
           T px[KPL], py[KPL], pz[KPL], ph[KPL];
 #pragma unroll
           for (int j = 0; j < KPL; ++j) {
@@ -673,6 +718,13 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         const int a = a0 + k;
         if (a >= L) break;
         const T S = warp_sum(hpc[k]);
+        if constexpr (SPLIT && PREC != kFP64) {
+          if (G > 1) {
+            // this warp's share of atom a's contact sum; the restraint comes after the combination
+            if (lane == 0) sp.gparts[sp.sub * sp.pstride + kPartTerms + a] = (float)S;
+            continue;
+          }
+        }
         const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
         const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
         ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
@@ -711,7 +763,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       if (cnt > 0) {
         const int beg = J.kbeg[lt];
         const T inv = (T)1 / (T)cnt;
-        for (int k = beg + lane; k < beg + cnt; k += 32) {
+        for (int k = beg + 32 * my_sub + lane; k < beg + cnt; k += 32 * G) {
           const float4 q = kde[GD_AT(k, J.nkde, kSiteKde)];
           T s = 0;
           for (int b = a; b < aend; ++b) {
@@ -730,6 +782,54 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   T ekde;
   if constexpr (PREC == kFP64) ekde = warp_sum(kacc) / (double)par->kde3;
   else ekde = warp_sum(kacc) * par->kde3_inv;
+
+  if constexpr (SPLIT && PREC != kFP64) {
+    if (G > 1) {
+      // one replica over G warps: publish this warp's partial sums, and let warp
+      // 0 of the group combine them in warp order (compensated for the dense
+      // terms with the FP32-Kahan policy) and finish the evaluation
+      float *mine = sp.gparts + sp.sub * sp.pstride;
+      if (lane == 0) {
+        mine[0] = vdw;
+        mine[1] = ele;
+        mine[2] = pmf;
+        mine[3] = psp;
+        mine[4] = hdb;
+        mine[5] = ekde;
+      }
+      group_sync(sp.bar_id, G);
+      if (sp.sub != 0) return;
+      float cv = 0.f, ce = 0.f, cp = 0.f;
+      for (int g = 1; g < G; ++g) {
+        const float *o = sp.gparts + g * sp.pstride;
+        if constexpr (PREC == kFP32Kahan) {
+          kahan_add(vdw, cv, o[0]);
+          kahan_add(ele, ce, o[1]);
+          kahan_add(pmf, cp, o[2]);
+        } else {
+          vdw += o[0];
+          ele += o[1];
+          pmf += o[2];
+        }
+        psp += o[3];
+        hdb += o[4];
+        ekde += o[5];
+      }
+      vdw += cv;
+      ele += ce;
+      pmf += cp;
+      // the hydrophobic restraint on each atom's combined contact sum (energy_prt_v1.cu:162-169)
+      float eh = 0.f;
+      for (int a = lane; a < L; a += 32) {
+        float S = sp.gparts[kPartTerms + a];
+        for (int g = 1; g < G; ++g) S += sp.gparts[g * sp.pstride + kPartTerms + a];
+        const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
+        const float h2 = (S - par->hpl0[lt]) / par->hpl1[lt];
+        eh += 0.5f * h2 * h2 - par->hpl2[lt];
+      }
+      ehpc = warp_sum(eh);
+    }
+  }
 
   // ---- MCS, energy_mcs_v1.cu:277-320
   T macc = 0;
@@ -776,6 +876,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   const T elhm = warp_sum(macc);
 
   // ---- distance to the pocket centre, kernel_cuda_l1_montecarlo.cu:439-454
+  const float *pc = J.pcenter + 3 * GD_AT(iprt, J.nprt, kSitePrtConf);
   T dst = 0;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -867,15 +968,18 @@ struct WarpStats {
   int pad_;
 };
 
-template <int MODE, int PREC, int KPL, int AB>
+template <int MODE, int PREC, int KPL, int AB, bool SPLIT = false>
 __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_item;
-  const SmemLayout sl = smem_layout(A.P, A.Kst, A.lig_slots, blockDim.x / 32, PREC == kFP64);
+  // G warps per replica (latency mode, the SPLIT instantiation): warp `sub` of replica slot `gi`
+  const int G = SPLIT ? kernel_group<MODE, PREC>(A) : 1;
+  const SmemLayout sl = smem_layout(A.P, A.Kst, A.lig_slots, blockDim.x / 32, PREC == kFP64, G);
   const int warp = threadIdx.x >> 5;
   const int lane = lane_id();
+  const int gi = warp / G, sub = warp - gi * G;
   // a Complex the device packer refused (gd_devpack.cu) leaves its job unread
   if (*(volatile int *)A.err & kErrPack) return;
   if (threadIdx.x == 0) mbar_init(&bar, 1);
@@ -920,14 +1024,20 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
                                 : J.aux + (size_t)wi.prt * J.npoint_pad;
     const float4 *kde = (J.nkde <= A.Kst) ? reinterpret_cast<const float4 *>(smem + sl.kde) : J.kde;
     const int2 *lgrp = reinterpret_cast<const int2 *>(smem + sl.lgrp);
+    // each warp rotates the ligand into its own buffer; the replica's state, its
+    // proposal and the evaluation's result live in the group's first warp
     unsigned char *wbase = smem + sl.warp0 + (size_t)warp * sl.warp_bytes;
+    unsigned char *gbase = smem + sl.warp0 + (size_t)(gi * G) * sl.warp_bytes;
     void *ligbuf = wbase;
-    ReplicaMC *srep = reinterpret_cast<ReplicaMC *>(wbase + sl.lig_bytes);
-    EnergyScratch *esc = reinterpret_cast<EnergyScratch *>(wbase + sl.lig_bytes + sizeof(ReplicaMC));
-    WarpStats *wst = reinterpret_cast<WarpStats *>(wbase + sl.lig_bytes + sizeof(ReplicaMC) + sizeof(EnergyScratch));
+    ReplicaMC *srep = reinterpret_cast<ReplicaMC *>(gbase + sl.lig_bytes);
+    EnergyScratch *esc = reinterpret_cast<EnergyScratch *>(gbase + sl.lig_bytes + sizeof(ReplicaMC));
+    WarpStats *wst = reinterpret_cast<WarpStats *>(gbase + sl.lig_bytes + sizeof(ReplicaMC) + sizeof(EnergyScratch));
+    typename std::conditional<SPLIT, Split, NoSplit>::type sp{};
+    if constexpr (SPLIT) sp = Split{sub, G, 1 + gi, reinterpret_cast<float *>(gbase + sl.parts), sl.warp_bytes / 4u};
+    const bool lead = sub == 0;  // the group's first warp: proposal, Metropolis, state
 
-    if (warp < wi.count) {
-      const int r = wi.rep0 + warp;  // job-local index
+    if (gi < wi.count) {
+      const int r = wi.rep0 + gi;  // job-local index
       if constexpr (MODE == 1) {
         // ---- pose evaluation
         const int ilig = A.conf[2 * r], iprt = A.conf[2 * r + 1];
@@ -944,8 +1054,8 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         // ---- Monte Carlo chunk for replica r
         const int gr = J.rid_base + r;
         int *sw = reinterpret_cast<int *>(srep);
-        sw[lane] = reinterpret_cast<const int *>(J.rep + GD_AT(r, J.nrep, kSiteRep))[lane];
-        if (lane == 0) {
+        if (lead) sw[lane] = reinterpret_cast<const int *>(J.rep + GD_AT(r, J.nrep, kSiteRep))[lane];
+        if (lead && lane == 0) {
           const RepStats &S = J.stats[r];
           wst->e_sum = 0.0;
           wst->e_sum2 = 0.0;
@@ -955,13 +1065,14 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
           for (int i = 0; i < 6; ++i) wst->best_mm[i] = S.best_mm[i];
         }
         __syncwarp();
+        if (G > 1) group_sync(1 + gi, G);  // the replica's state is in shared memory
         int acc = J.run_acc[r];
         const int ilig = srep->idx_lig, iprt = srep->idx_prt;
         const double mbeta = (double)J.minus_beta[GD_AT(srep->idx_tmp, J.ntmp, kSiteTmp)];
         Record *rec = (J.rec && (A.flags & kMcRecord)) ? J.rec + r : nullptr;
         int ne = 0;
         if (J.rec && (A.flags & kMcResetRecord)) {
-          if (lane == 0) J.rec[r].next_entry = 0;
+          if (lead && lane == 0) J.rec[r].next_entry = 0;
         } else if (rec) {
           ne = rec->next_entry;
         }
@@ -970,7 +1081,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
         const int s0 = (A.d_step ? *A.d_step + A.s_begin : A.s_begin) + J.step0;
         const int nsteps = J.nsteps > 0 ? min(J.nsteps, A.nsteps) : A.nsteps;
         for (int s = s0; s < s0 + nsteps; ++s) {
-          if (acc) {
+          if (acc && lead) {
             // record the old state, kernel_cuda_l1_montecarlo.cu:290-297
             if (lane == 0) srep->step = s;
             __syncwarp();
@@ -980,7 +1091,9 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
           // draws of step s: counter {s, replica, 0, 0} -> move x y z, rot x;
           // {s, replica, 0, 1} -> rot y z, accept (lane 0 and lane 1 compute one each)
           float u_acc = 0.0f;
-          if (!initial) {
+          if (!lead) {
+            // the proposal is the group's first warp's
+          } else if (!initial) {
             const Philox4 d = philox4x32_10((uint32_t)s, (uint32_t)gr, 0u, (uint32_t)(lane & 1), J.key0, J.key1);
             float u[7];
 #pragma unroll
@@ -998,7 +1111,10 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
             esc->mm[lane] = __fmaf_rn(par->move_scale[lane], 0.0f, srep->movematrix[lane]);
           }
           __syncwarp();
-          energy_warp<PREC, KPL, AB>(J, par, pos, aux, kde, lgrp, apt, aph, ahd, ligbuf, ilig, iprt, esc->mm, esc);
+          if (G > 1) group_sync(1 + gi, G);  // the proposal is in shared memory
+          energy_warp<PREC, KPL, AB, SPLIT>(J, par, pos, aux, kde, lgrp, apt, aph, ahd, ligbuf, ilig, iprt, esc->mm, esc,
+                                            sp);
+          if (!lead) continue;  // the group's first warp holds the result
           const float etot = (float)esc->e[9];
 
           // Metropolis test in FP64, kernel_cuda_l1_montecarlo.cu:485-507
@@ -1027,21 +1143,23 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
           acc = accept;
         }
 
-        if (lane == 0) {
-          J.run_acc[r] = acc;
-          if (A.flags & kMcStoreAccept) srep->is_accept = acc;
-          if (rec) rec->next_entry = ne;
-          RepStats &S = J.stats[r];
-          S.e_sum += wst->e_sum;
-          S.e_sum2 += wst->e_sum2;
-          S.n_steps += nsteps;
-          S.n_accept += wst->n_acc;
-          S.best_e = wst->best_e;
-          S.best_step = wst->best_step;
-          for (int i = 0; i < 6; ++i) S.best_mm[i] = wst->best_mm[i];
+        if (lead) {
+          if (lane == 0) {
+            J.run_acc[r] = acc;
+            if (A.flags & kMcStoreAccept) srep->is_accept = acc;
+            if (rec) rec->next_entry = ne;
+            RepStats &S = J.stats[r];
+            S.e_sum += wst->e_sum;
+            S.e_sum2 += wst->e_sum2;
+            S.n_steps += nsteps;
+            S.n_accept += wst->n_acc;
+            S.best_e = wst->best_e;
+            S.best_step = wst->best_step;
+            for (int i = 0; i < 6; ++i) S.best_mm[i] = wst->best_mm[i];
+          }
+          __syncwarp();
+          reinterpret_cast<int *>(J.rep + r)[lane] = sw[lane];
         }
-        __syncwarp();
-        reinterpret_cast<int *>(J.rep + r)[lane] = sw[lane];
       }
     }
     __syncthreads();
@@ -1180,16 +1298,19 @@ cudaError_t launch_eval_global(int precision, const DevJob *d_job, const int *co
 }
 
 // ---------------------------------------------------------- launchers --
-size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision)
+size_t kernel_smem_bytes(int P, int Kst, int lig_slots, int warps, int precision, int group)
 {
-  return smem_layout(P, Kst, lig_slots, warps, precision == kFP64).total;
+  return smem_layout(P, Kst, lig_slots, warps, precision == kFP64, group).total;
 }
 
 template <int MODE, int PREC, int KPL, int AB>
 static cudaError_t launch_t(const KArgs &a, int warps, int grid, cudaStream_t st)
 {
-  const size_t smem = kernel_smem_bytes(a.P, a.Kst, a.lig_slots, warps, PREC);
-  auto k = mc_kernel<MODE, PREC, KPL, AB>;
+  const int group = kernel_group<MODE, PREC>(a);
+  const size_t smem = kernel_smem_bytes(a.P, a.Kst, a.lig_slots, warps, PREC, group);
+  auto k = mc_kernel<MODE, PREC, KPL, AB, false>;
+  if constexpr (MODE == 0 && PREC != kFP64 && KPL % 2 == 0)
+    if (group > 1) k = mc_kernel<MODE, PREC, KPL, AB, true>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, warps * 32, smem, st>>>(a);
@@ -1224,8 +1345,11 @@ cudaError_t launch_kernel(int mode, int precision, const TileConfig &tc, const K
 int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem)
 {
   const void *f = nullptr;
+  const bool split = mode == 0 && precision != kFP64 && tc.group > 1;
 #define GD_PICK(M, PR, K, A)                                                                  \
-  if (mode == M && precision == PR && tc.kpl == K && tc.ab == A) f = (const void *)mc_kernel<M, PR, K, A>;
+  if (mode == M && precision == PR && tc.kpl == K && tc.ab == A)                              \
+    f = split ? (const void *)mc_kernel<M, PR, K, A, (M == 0 && PR != kFP64 && K % 2 == 0)> \
+              : (const void *)mc_kernel<M, PR, K, A, false>;
 #define GD_PICK_ALL(M, PR) GD_PICK(M, PR, 1, 8) GD_PICK(M, PR, 2, 4) GD_PICK(M, PR, 2, 8) GD_PICK(M, PR, 4, 4)
   GD_PICK_ALL(0, kFP32) GD_PICK_ALL(0, kFP32Kahan) GD_PICK_ALL(0, kFP64)
   GD_PICK_ALL(1, kFP32) GD_PICK_ALL(1, kFP32Kahan) GD_PICK_ALL(1, kFP64)

@@ -212,7 +212,7 @@ void complete(gd_server *s, std::vector<ServeReq *> &done)
 // conformation, at most warps_per_cta long, heaviest job first.
 void append_items(const gd_server *s, const ServeReq &r, std::vector<WorkItem> &out)
 {
-  const int R = s->tc.warps_per_cta;
+  const int R = s->tc.warps_per_cta / s->tc.group;  // replicas per CTA
   const std::vector<ReplicaMC> &reps = r.jd.reps;
   int i = 0;
   while (i < r.nrep) {
@@ -281,6 +281,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   a.P = s->tc.stage ? s->Pmax : 0;
   a.Kst = s->Kst;
   a.lig_slots = s->lig_slots;
+  a.group = s->tc.group;
   int launches = 0;
   GD_CUDA(cudaEventRecord(s->t_ev[b][0], s->st));
   if (any_fresh) {
@@ -465,22 +466,24 @@ int server_configure(gd_server *s)
 {
   int nsm = 0;
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device));
-  const int w0 = s->cfg.warps, wlo = w0 > 0 ? w0 : 2, whi = w0 > 0 ? w0 : kMaxCtaThreads / 32;
+  const int G = s->tc.group;
+  const int w0 = s->cfg.warps, wlo = w0 > 0 ? w0 : std::max(2, G), whi = w0 > 0 ? w0 : kMaxCtaThreads / 32;
   int best_w = 0, best_res = 0, best_occ = 0, best_kst = 0, best_stage = 1;
   size_t best_smem = 0;
   // resident replica-warps per SM decide; the pocket is staged in shared
   // memory unless reading it through L1 lets more replicas be resident
   for (int stage = 1; stage >= 0; --stage)
   for (int w = wlo; w <= whi; ++w) {
+    if (w % G) continue;
     TileConfig tc = s->tc;
     tc.warps_per_cta = w;
     tc.stage = stage;
     const int P = stage ? s->Pmax : 0;
     int kst = s->cfg.kde_stage;
-    size_t smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision);
+    size_t smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision, G);
     if (smem > kSmemLimitServe) {
       kst = 0;
-      smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision);
+      smem = kernel_smem_bytes(P, kst, s->lig_slots, w, s->precision, G);
     }
     if (smem > kSmemLimitServe) continue;
     const int occ = kernel_occupancy(0, s->precision, tc, smem);
@@ -503,7 +506,7 @@ int server_configure(gd_server *s)
   s->grid = best_occ * nsm;
   // four waves of resident replica-warps per round: more balanced rounds (items
   // of uneven jobs) than two, with the same latency below saturation
-  if (s->cfg.max_active_replicas <= 0) s->cfg.max_active_replicas = 4 * best_occ * nsm * best_w;
+  if (s->cfg.max_active_replicas <= 0) s->cfg.max_active_replicas = 4 * best_occ * nsm * (best_w / G);
   return GD_OK;
 }
 
@@ -548,7 +551,11 @@ int server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *e
   const long long o_kpl = gd_get_option("kpl"), o_ab = gd_get_option("ab");
   s->precision = (int)gd_get_option("precision");
   s->tc = TileConfig{8, (int)o_kpl, (int)o_ab};
-  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8;
+  s->tc.group = s->cfg.replica_warps > 0 ? s->cfg.replica_warps : 1;
+  if (s->tc.group != 1 && s->tc.group != 2 && s->tc.group != 4 && s->tc.group != 8)
+    return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8)", s->cfg.replica_warps);
+  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1;
+  if (s->tc.kpl % 2) s->tc.group = 1;  // the split form exists for the FP32 atom-pair loop
   GD_TRY(server_configure(s));
   s->max_items = s->cfg.max_active_replicas * 2 + s->cfg.max_replicas_per_job;
   GD_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
@@ -597,6 +604,7 @@ void gd_server_config_default(gd_server_config_t *cfg)
   cfg->steps_per_round = 50;
   cfg->kde_stage = 0;  // FP32 reads the KDE points through L1
   cfg->warps = 0;
+  cfg->replica_warps = 1;
   cfg->device = 0;
 }
 

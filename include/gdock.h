@@ -293,8 +293,10 @@ typedef struct gd_server_config {
   int max_atoms;            /* largest ligand accepted (sizes the per-warp buffers), default 128 */
   int steps_per_round;      /* MC steps between scheduling decisions, default 50 */
   int kde_stage;            /* KDE points staged in shared memory (more: read through L1), default 0 */
-  int warps;                /* replicas per CTA, 0: occupancy model */
+  int warps;                /* warps per CTA, 0: occupancy model */
   int device;
+  int replica_warps;        /* warps per replica, 1 (default), 2, 4 or 8: latency mode, every
+                               replica's pair rows and KDE points split over that many warps */
 } gd_server_config_t;
 
 typedef struct gd_request {

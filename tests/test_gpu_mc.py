@@ -495,3 +495,52 @@ def test_restore_refuses_other_seed(lib, enepara):
         assert ei.value.code == GD_E_INVALID
         with pytest.raises(GdockError):
             b.restore(b"not a snapshot" * 4)
+
+
+@pytest.mark.parametrize("g", [2, 4, 8])
+def test_replica_warps_matches_oracle(lib, enepara, oracle_lib, g):
+    """Latency mode: every replica split over g warps (pair rows, KDE points and
+    hydrophobic sums divided, partials combined in warp order).  The chains
+    follow the FP64 oracle's as the one-warp form does, and the result does not
+    depend on how many replicas share a CTA (only on g)."""
+    cx = _small_ensemble(enepara, seed=31, L=27, P=450)
+    n = int(cx[0]["size"]["n_rep"])
+    ref = _oracle_run(oracle_lib, cx, 3, 120, spx=20)
+    res = {}
+    try:
+        check(lib.gd_set_option(b"replica_warps", g))
+        for w in (g, 2 * g):
+            check(lib.gd_set_option(b"warps", w))
+            with dock.Ensemble.from_complexes([cx], [3]) as ens:
+                ens.init()
+                ens.run(120, 20)
+                ens.sync()
+                res[w] = ens.replicas(0)
+    finally:
+        check(lib.gd_set_option(b"replica_warps", 1))
+        check(lib.gd_set_option(b"warps", 0))
+    got, want = res[g], ref[0]["replica"][:n]
+    same = _same_trajectory(got, want)
+    assert same.mean() >= 0.9, same.mean()
+    _close(got["energy"][same], want["energy"][same])
+    for f in got.dtype.names:
+        assert res[2 * g][f].tobytes() == got[f].tobytes(), f
+
+
+def test_replica_warps_single_replica_trajectory(lib, enepara, oracle_lib):
+    """One replica over 8 warps follows the oracle's chain for 300 steps."""
+    pk, job = synth.config1(1)
+    cx = synth.to_complex(job, pk, enepara)
+    ref = _oracle_run(oracle_lib, cx, 7, 300)
+    try:
+        check(lib.gd_set_option(b"replica_warps", 8))
+        with dock.Ensemble.from_complexes([cx], [7]) as ens:
+            ens.init()
+            ens.run(300)
+            ens.sync()
+            got = ens.replicas(0)
+    finally:
+        check(lib.gd_set_option(b"replica_warps", 1))
+    want = ref[0]["replica"][:1]
+    assert _same_trajectory(got, want).all()
+    _close(got["energy"], want["energy"])

@@ -181,3 +181,26 @@ def test_injected_allocation_failure(lib, enepara):
     assert res[t1]["status"] == GD_E_NOMEM
     assert res[t2]["status"] == 0 and res[t3]["status"] == 0
     assert st["failed"] == 1 and st["completed"] == 2 and st["used_bytes"] == 0
+
+
+def test_latency_mode_same_alone_and_in_mix(lib, enepara):
+    """A server in latency mode (4 warps per replica): each request's result is
+    the same, bit for bit, alone and in a mix of requests that arrive while it
+    runs, and within the parity tolerance of the one-warp ensemble path."""
+    pockets = _pockets()
+    jobs = _jobs(pockets, 4, seed=9)
+    reqs = [(jobs[0], 100, 25), (jobs[1], 60, 20), (jobs[2], 80, 40), (jobs[3], 50, 50)]
+    alone = [_serve(pockets, enepara, [r], replica_warps=4)[0][0] for r in reqs[:2]]
+    mix, st = _serve(pockets, enepara, reqs, stagger_s=0.005, replica_warps=4)
+    for a, b in zip(alone, mix[:2]):
+        assert a["status"] == 0 and b["status"] == 0
+        for f in a["replicas"].dtype.names:
+            assert a["replicas"][f].tobytes() == b["replicas"][f].tobytes(), f
+    from oracle import tolerance as TOL
+
+    job, steps, spx = reqs[0]
+    want, _ = _ensemble_result(pockets, job, enepara, steps, spx)
+    got = mix[0]["replicas"]
+    same = np.all(got["movematrix"] == want["movematrix"], axis=1)
+    assert same.mean() >= 0.9
+    assert np.all(TOL.scaled_error(got["energy"][same], want["energy"][same]) <= 1.0)
