@@ -367,7 +367,6 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
 {
   KArgs a{};
   a.jobs = e->d_jobs;
-  a.n_jobs = (int)e->jobs.size();
   a.items = e->d_items;
   a.n_items = e->n_items;
   a.queue = e->d_queue;
@@ -379,9 +378,9 @@ KArgs mc_args(gd_ensemble *e, int s_begin, int nsteps, int flags, const int *d_s
   a.P = e->tc.stage ? e->Pmax : 0;
   a.Kst = e->Kst;
   a.lig_slots = e->lig_slots;
-  a.group = e->tc.group;
+  a.group = (uint16_t)e->tc.group;
   a.wait_limit = e->wait_limit;
-  a.stall_bytes = e->stall_bytes;
+  a.stall_bytes = (uint16_t)e->stall_bytes;
   return a;
 }
 
@@ -1088,7 +1087,6 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
   EV_CUDA(cudaMemsetAsync(e->d_queue, 0, sizeof(int), e->st));
   KArgs a{};
   a.jobs = e->d_jobs;
-  a.n_jobs = (int)e->jobs.size();
   a.items = d_items;
   a.n_items = (int)items.size();
   a.queue = e->d_queue;

@@ -196,17 +196,17 @@ struct KArgs {
   const int *d_step;       // if set, steps start at *d_step + s_begin (graph replay)
   int P, Kst, lig_slots;   // smem layout (maxima over the launched jobs); P = 0: pocket read from global memory
   uint32_t wait_limit;     // microseconds a bounded shared-memory wait lasts before it gives up (0: one second)
-  uint32_t stall_bytes;    // test hook: bytes announced to the staging barrier that no copy delivers, so
+  uint16_t stall_bytes;    // test hook: bytes announced to the staging barrier that no copy delivers, so
                            // that its bounded wait runs out (0 in normal use)
+  uint16_t group;          // warps per replica (TileConfig::group); 0 reads as 1.  Two 16-bit fields in the
+                           // place of one 32-bit one: the size of this struct changes the kernels' register
+                           // allocation (measured), so it is kept
   // pose evaluation
   const int *conf;
   const float *mm;
   float *out;
   double *out64;
   float *raw;
-  // (after the fields above, whose offsets the kernels' register allocation turned out to depend on)
-  int n_jobs;              // entries of jobs (the work items' job indices are below it)
-  int group;               // warps per replica (TileConfig::group); 0 reads as 1
 };
 
 // Shared-memory bytes of the batched kernel for pocket conformations of P

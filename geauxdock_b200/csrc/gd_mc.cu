@@ -105,7 +105,7 @@ __device__ __forceinline__ long long check_at(long long i, long long n, int site
 #endif
 // sites reported by gd_check_report
 enum CheckSite { kSiteLig = 1, kSiteApt, kSiteAph, kSiteAhd, kSitePos, kSitePsp, kSiteKde, kSiteMcs, kSiteLgrp,
-                 kSiteTcc, kSiteLigConf, kSitePrtConf, kSiteRep, kSiteTmp, kSiteJob, kSiteTab, kSiteTrng };
+                 kSiteTcc, kSiteLigConf, kSitePrtConf, kSiteRep, kSiteTmp, kSiteTab = 16 };
 
 // ----------------------------------------------------------- smem layout --
 struct SmemLayout {
@@ -114,7 +114,7 @@ struct SmemLayout {
 
 // Per-warp partial sums of a replica split over several warps (latency mode):
 // the dense terms, then the hydrophobic sum of every atom.
-constexpr int kPartTerms = 8;    // vdw, ele, pmf, psp, hdb, kde, (2 unused)
+constexpr int kPartTerms = 8;    // vdw, ele, pmf, psp, hdb, kde, mcs, (1 unused)
 constexpr uint32_t kPartBytes = 4u * (kPartTerms + kMaxAtoms);
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
@@ -752,18 +752,20 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   // ---- KDE, energy_kde_v1.cu:183-274: per atom, mean of exp(kde2 d^2) over
   // the KDE points of the same type; atoms with no such point contribute 0.
   // One type group at a time: lane k holds KDE point k of the group's type and
-  // sums over the group's atoms, then scales by 1 / (points of the type).
+  // sums over the group's atoms, then scales by 1 / (points of the type).  A
+  // replica split over G warps deals the type groups out to its warps in turn.
   T kacc = 0;
   {
     const T kde2 = par->kde2;
-    for (int a = 0; a < L;) {
+    int tg = 0;
+    for (int a = 0; a < L; ++tg) {
       const int2 grp = lgrp[GD_AT(a, L, kSiteLgrp)];
       const int lt = GD_AT(grp.x, kLigTypes, kSiteTab), aend = grp.y;
       const int cnt = J.kcnt[lt];
-      if (cnt > 0) {
+      if (cnt > 0 && (G == 1 || tg % G == my_sub)) {
         const int beg = J.kbeg[lt];
         const T inv = (T)1 / (T)cnt;
-        for (int k = beg + 32 * my_sub + lane; k < beg + cnt; k += 32 * G) {
+        for (int k = beg + lane; k < beg + cnt; k += 32) {
           const float4 q = kde[GD_AT(k, J.nkde, kSiteKde)];
           T s = 0;
           for (int b = a; b < aend; ++b) {
@@ -783,19 +785,67 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   if constexpr (PREC == kFP64) ekde = warp_sum(kacc) / (double)par->kde3;
   else ekde = warp_sum(kacc) * par->kde3_inv;
 
+
+  // ---- MCS, energy_mcs_v1.cu:277-320
+  T macc = 0;
+  {
+    const int M = J.nmcs;
+    if (M <= 16) {
+      // two half-warps share each template: lane and lane + 16 take its even and odd atoms
+      const int m = lane & 15, h = lane >> 4;
+      T s = 0;
+      int n = 0;
+      // a replica split over G warps deals the templates out to its warps
+      const bool mine = m < M && (G == 1 || m % G == my_sub);
+      if (mine) {
+        for (int a = h; a < L; a += 2) {
+          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
+          if (q.w != 0.0f) {
+            const V4<T> la = atom_at(lig, a);
+            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+            s += dx * dx + dy * dy + dz * dz;
+            ++n;
+          }
+        }
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 16);
+      n += __shfl_xor_sync(0xffffffffu, n, 16);
+      if (mine && h == 0) macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
+    } else
+    for (int m0 = 32 * my_sub; m0 < M; m0 += 32 * G) {
+      const int m = m0 + lane;
+      if (m < M) {
+        T s = 0;
+        int n = 0;
+        for (int a = 0; a < L; ++a) {
+          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
+          if (q.w != 0.0f) {
+            const V4<T> la = atom_at(lig, a);
+            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
+            s += dx * dx + dy * dy + dz * dz;
+            ++n;
+          }
+        }
+        macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
+      }
+    }
+  }
+  T elhm = warp_sum(macc);
+
   if constexpr (SPLIT && PREC != kFP64) {
     if (G > 1) {
       // one replica over G warps: publish this warp's partial sums, and let warp
       // 0 of the group combine them in warp order (compensated for the dense
       // terms with the FP32-Kahan policy) and finish the evaluation
-      float *mine = sp.gparts + sp.sub * sp.pstride;
+      float *part = sp.gparts + sp.sub * sp.pstride;
       if (lane == 0) {
-        mine[0] = vdw;
-        mine[1] = ele;
-        mine[2] = pmf;
-        mine[3] = psp;
-        mine[4] = hdb;
-        mine[5] = ekde;
+        part[0] = vdw;
+        part[1] = ele;
+        part[2] = pmf;
+        part[3] = psp;
+        part[4] = hdb;
+        part[5] = ekde;
+        part[6] = elhm;
       }
       group_sync(sp.bar_id, G);
       if (sp.sub != 0) return;
@@ -814,6 +864,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         psp += o[3];
         hdb += o[4];
         ekde += o[5];
+        elhm += o[6];
       }
       vdw += cv;
       ele += ce;
@@ -830,50 +881,6 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       ehpc = warp_sum(eh);
     }
   }
-
-  // ---- MCS, energy_mcs_v1.cu:277-320
-  T macc = 0;
-  {
-    const int M = J.nmcs;
-    if (M <= 16) {
-      // two half-warps share each template: lane and lane + 16 take its even and odd atoms
-      const int m = lane & 15, h = lane >> 4;
-      T s = 0;
-      int n = 0;
-      if (m < M) {
-        for (int a = h; a < L; a += 2) {
-          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
-          if (q.w != 0.0f) {
-            const V4<T> la = atom_at(lig, a);
-            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
-            s += dx * dx + dy * dy + dz * dz;
-            ++n;
-          }
-        }
-      }
-      s += __shfl_xor_sync(0xffffffffu, s, 16);
-      n += __shfl_xor_sync(0xffffffffu, n, 16);
-      if (m < M && h == 0) macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
-    } else
-    for (int m0 = 0; m0 < M; m0 += 32) {
-      const int m = m0 + lane;
-      if (m < M) {
-        T s = 0;
-        int n = 0;
-        for (int a = 0; a < L; ++a) {
-          const float4 q = J.mcs[GD_AT((size_t)a * M + m, (size_t)L * M, kSiteMcs)];
-          if (q.w != 0.0f) {
-            const V4<T> la = atom_at(lig, a);
-            const T dx = la.x - (T)q.x, dy = la.y - (T)q.y, dz = la.z - (T)q.z;
-            s += dx * dx + dy * dy + dz * dz;
-            ++n;
-          }
-        }
-        macc += (T)J.tcc[GD_AT(m, M, kSiteTcc)] * sqrt(s / (T)n);
-      }
-    }
-  }
-  const T elhm = warp_sum(macc);
 
   // ---- distance to the pocket centre, kernel_cuda_l1_montecarlo.cu:439-454
   const float *pc = J.pcenter + 3 * GD_AT(iprt, J.nprt, kSitePrtConf);
@@ -993,7 +1000,7 @@ __global__ void __maxnreg__(PREC == kFP64 ? 128 : 80) mc_kernel(KArgs A)
     const int it = s_item;
     if (it >= A.n_items) break;
     const WorkItem wi = A.items[it];
-    const DevJob &J = A.jobs[GD_AT(wi.job, A.n_jobs, kSiteJob)];
+    const DevJob &J = A.jobs[wi.job];
     if (wi.job != prev_job || wi.prt != prev_prt) {
       if (!stage_item<PREC == kFP64>(A, J, wi, smem, sl, &bar, phase)) {
         if (threadIdx.x == 0) atomicOr(A.err, kErrTimeout);

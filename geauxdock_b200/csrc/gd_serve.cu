@@ -275,13 +275,12 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
                           s->st));
   KArgs a{};
   a.jobs = s->d_jobs;
-  a.n_jobs = nslot;
   a.queue = s->d_queue;
   a.err = s->d_err;
   a.P = s->tc.stage ? s->Pmax : 0;
   a.Kst = s->Kst;
   a.lig_slots = s->lig_slots;
-  a.group = s->tc.group;
+  a.group = (uint16_t)s->tc.group;
   int launches = 0;
   GD_CUDA(cudaEventRecord(s->t_ev[b][0], s->st));
   if (any_fresh) {

@@ -25,7 +25,7 @@ from oracle import oracle as O, tolerance as TOL  # noqa: E402
 
 SITES = ["", "ligand pair", "pair table", "H-bond table", "pair header", "pocket point", "pocket potential",
          "KDE point", "MCS template", "type group", "MCS weight", "ligand conformation", "protein conformation",
-         "replica", "temperature", "job", "type table", "type range"]
+         "replica", "temperature", "", "type table"]
 
 
 def report(lib):
