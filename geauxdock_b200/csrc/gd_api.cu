@@ -488,6 +488,7 @@ int ensemble_from_complex_range(const Complex *c, int rb, int re, uint64_t seed,
   JobData jd;
   GD_TRY(pocket_from_complex(c, pk));
   GD_TRY(job_from_complex(c, rb, re, seed, jd));
+  jd.cell_room = true;  // Dock refills this state in place from later Complexes
   tr.mark("read Complex");
   gd_ensemble *e = new gd_ensemble;
   e->device = device;
@@ -561,6 +562,9 @@ int dock_refill_device(gd_ensemble *e, const Complex *d_cx, int rb, int re, int 
   D.ncdc = pk.ncdc;
   D.psp = const_cast<float *>(J.psp);
   D.pspmask = const_cast<uint32_t *>(J.pspmask);
+  D.pcell = const_cast<int4 *>(J.pcell);
+  D.pcell_cnt = const_cast<int *>(J.pcell_cnt);
+  D.pcell_stride = J.pcell_stride;
   D.kde_cap = std::max(J.nkde, 1);
   D.Ppad = pk.Ppad;
   D.nkde_expect = J.nkde;
@@ -624,6 +628,7 @@ int dock_ensemble(gd_rng *h, const Complex *c, const Complex *d_cx, int rb, int 
     GD_CUDA(cudaStreamSynchronize(e->st));
     JobData jd;
     GD_TRY(job_from_complex(c, rb, re, seed, jd));
+    jd.cell_room = true;  // the arena keeps the size of the one it refills
     bool ok = true;
     const bool same_prt =
         h->dock_prt.size() == prt_bytes && std::memcmp(h->dock_prt.data(), c->prt, prt_bytes) == 0;

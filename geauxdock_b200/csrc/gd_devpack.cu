@@ -239,6 +239,9 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
     J.pcenter = D.pcenter;
     J.psp = D.psp;
     J.pspmask = D.pspmask;
+    J.pcell = D.pcell;
+    J.pcell_cnt = D.pcell_cnt;
+    J.pcell_stride = D.pcell_stride;
     for (int t = 0; t < kLigTypes; ++t) {
       J.kbeg[t] = s_kbeg[t];
       J.kcnt[t] = s_kcnt[t];
@@ -272,8 +275,9 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
 // One CTA per protein conformation: points ordered as the host packer orders
 // them (hydrophobic-contact points first, each part sorted by point type,
 // stable; 60 buckets (cdc, type), two per warp, counted and scattered with
-// warp ballots), inert padding, and the pocket-specific potential gathered
-// with its non-zero type mask.
+// warp ballots), inert padding, the pocket-specific potential gathered with
+// its non-zero type mask, and its non-zero cells for the ligand's types, by
+// type then point (one warp per type, counted and scattered the same way).
 __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restrict__ cx, PackDst D)
 {
   constexpr int kBuckets = 2 * kPadType;
@@ -341,6 +345,50 @@ __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restri
     aux[j] = make_float2(0.f, dp_as_float(kPadType));
     pm[j] = 0u;
     for (int lt = 0; lt < kLigTypes; ++lt) psp[(size_t)lt * Pp + j] = 0.f;
+  }
+  if (!D.pcell) return;
+  // cells: the atoms of type t are [tbeg, tbeg + tcnt) of the type-grouped ligand
+  __shared__ int s_tcnt[kLigTypes], s_tbeg[kLigTypes], s_ccnt[kLigTypes], s_cbeg[kLigTypes];
+  __syncthreads();  // this CTA's mask writes above are read below
+  const int L = cx->lig[0].lig_natom;
+  if (warp < kLigTypes) {
+    int na = 0;
+    for (int a0 = 0; a0 < L; a0 += 32)
+      na += __popc(__ballot_sync(0xffffffffu, a0 + lane < L && cx->lig[0].t2[a0 + lane] == warp));
+    int nc = 0;
+    if (na > 0)
+      for (int j0 = 0; j0 < Pp; j0 += 32)
+        nc += __popc(__ballot_sync(0xffffffffu, j0 + lane < Pp && ((pm[j0 + lane] >> warp) & 1u)));
+    if (lane == 0) {
+      s_tcnt[warp] = na;
+      s_ccnt[warp] = nc;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a = 0, c = 0;
+    for (int t = 0; t < kLigTypes; ++t) {
+      s_tbeg[t] = a;
+      s_cbeg[t] = c;
+      a += s_tcnt[t];
+      c += s_ccnt[t];
+    }
+    D.pcell_cnt[i] = min(c, D.pcell_stride);
+    if (c > D.pcell_stride) dp_fail(D, kPackFailCapacity, kFieldPcell, c);
+  }
+  __syncthreads();
+  if (warp < kLigTypes && s_tcnt[warp] > 0) {
+    int4 *cell = D.pcell + (size_t)i * D.pcell_stride;
+    const int t = warp, rng = s_tbeg[t] | ((s_tbeg[t] + s_tcnt[t]) << 16);
+    int at = s_cbeg[t];
+    for (int j0 = 0; j0 < Pp; j0 += 32) {
+      const int j = j0 + lane;
+      const bool m = j < Pp && ((pm[j] >> t) & 1u);
+      const unsigned b = __ballot_sync(0xffffffffu, m);
+      const int o = at + __popc(b & ((1u << lane) - 1u));
+      if (m && o < D.pcell_stride) cell[o] = make_int4(j, rng, __float_as_int(psp[(size_t)t * Pp + j]), t);
+      at += __popc(b);
+    }
   }
 }
 
@@ -427,6 +475,7 @@ const char *pack_field_name(int f)
     case kFieldP1a: return "enepara.p1a <= 0 (index lt * 32 + pt given; the pair kernel needs p1a > 0)";
     case kFieldNTmp: return "size.n_tmp (temperatures)";
     case kFieldReplica: return "a replica's conformation or temperature index (replica given)";
+    case kFieldPcell: return "non-zero pocket-specific cells of a conformation";
     default: return "unknown field";
   }
 }

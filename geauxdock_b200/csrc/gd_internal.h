@@ -20,7 +20,9 @@
 //                        per-type ranges
 //   MCS templates        mcs[L][M] float4 (x, y, z, valid), atom-major
 //   pocket potential     psp[prt conf][24][P] pre-gathered per sorted point,
-//                        pspmask[prt conf][P] its non-zero ligand types
+//                        pspmask[prt conf][P] its non-zero ligand types, and
+//                        pcell[prt conf][] its non-zero cells for the ligand's
+//                        types (the atom-pair pair loop's form)
 //
 // Every array a CTA stages into shared memory is a multiple of 16 bytes and
 // starts 16-byte aligned, so it can be copied with one 1-D bulk (TMA) copy.
@@ -118,6 +120,13 @@ struct DevJob {
   const float *pcenter;    // [nprt][3] pocket centre
   const float *psp;        // [nprt][24][npoint_pad]
   const uint32_t *pspmask; // [nprt][npoint_pad] bit t set where psp[.][t][p] != 0
+  // the same potential as a list of its non-zero cells (sorted point p, ligand type t) per
+  // conformation, for the types the ligand has, ordered by type, then point: cell k <
+  // pcell_cnt[c] of conformation c is pcell[c * pcell_stride + k] = (p, beg | end << 16,
+  // bits of the value, t), [beg, end) the atoms of type t in the type-grouped ligand
+  const int4 *pcell;
+  const int *pcell_cnt;    // [nprt]
+  int pcell_stride;
   // KDE
   int nkde;
   const float4 *kde;       // [nkde]

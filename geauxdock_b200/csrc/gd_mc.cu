@@ -477,13 +477,15 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
   if constexpr (PREC != kFP64 && KPL % 2 == 0) {
     // atom-pair form: atoms 2i and 2i+1 share one register pair and the
     // table entries come per atom pair, so there is no loop over type groups
+    // (the pocket-specific term is not in this loop: it walks the potential's
+    // non-zero cells after it)
     const LigPair *lp = lig;
     const int npairs = (L + 1) >> 1;
     for (int row = row0; row < P; row += rstep) {
       float2 npx[KPL], npy[KPL], npz[KPL];
       int pt[KPL];
       uint32_t pm[KPL];
-      uint32_t ptbits = 0u, pmbits = 0u;
+      uint32_t ptbits = 0u;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
         const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
@@ -492,15 +494,12 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         npy[j] = f2(-q.y);
         npz[j] = f2(-q.z);
         pt[j] = __float_as_int(aux[p].y);
-        pm[j] = __ldg(pmc + p);
+        pm[j] = 0u;
         ptbits |= 1u << pt[j];
-        pmbits |= pm[j];
       }
-      // point types present in the row, and ligand types with a pocket-specific
-      // potential on some point of it: decide per atom pair, for the whole warp,
-      // whether the sparse terms are evaluated
+      // point types present in the row: decide per atom pair, for the whole
+      // warp, whether the hydrogen-bond term is evaluated
       ptbits = __reduce_or_sync(0xffffffffu, ptbits);
-      pmbits = __reduce_or_sync(0xffffffffu, pmbits);
       PairAccP<KPL> acc;
       acc.vdw = acc.pmf = acc.hdb = f2(0.0f);
 #pragma unroll
@@ -509,20 +508,12 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       for (int i = 0; i < npairs; ++i) {
         const int2 fl = *reinterpret_cast<const int2 *>(&ahd[GD_AT(i, npairs, kSiteAhd)].x);
         const bool any_hdb = ((uint32_t)fl.x & ptbits) != 0u;
-        const bool any_psp = ((uint32_t)fl.y & pmbits) != 0u;
         const float4 l01 = *reinterpret_cast<const float4 *>(&lp[GD_AT(i, npairs, kSiteLig)].x);
         const float2 lx = make_float2(l01.x, l01.y), ly = make_float2(l01.z, l01.w), lz = lp[i].z;
-        if (any_hdb) {
-          if (any_psp)
-            pair_atom_pair<KPL, true, true>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
-          else
-            pair_atom_pair<KPL, true, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
-        } else {
-          if (any_psp)
-            pair_atom_pair<KPL, false, true>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
-          else
-            pair_atom_pair<KPL, false, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
-        }
+        if (any_hdb)
+          pair_atom_pair<KPL, true, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+        else
+          pair_atom_pair<KPL, false, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
       }
       float row_ele = 0.f;
 #pragma unroll
@@ -545,6 +536,39 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         s_psp += acc.psp;
         s_hdb += row_hdb;
       }
+    }
+    // Pocket-specific term (energy_prt_v1.cu:109-115) over the conformation's
+    // non-zero cells (point p, ligand type t, value v; only types the ligand
+    // has), ordered by type: lane k takes cell k and counts the atoms of type t
+    // (the contiguous range [beg, end) of the type-grouped ligand) with
+    // d - pmf0 <= 0.  d, -pmf0 (from the same pair table) and the comparison are
+    // the pair loop's operations in the same order, so an atom counts here
+    // exactly where that loop would count it.
+    {
+      const int4 *cell = J.pcell + (size_t)iprt * J.pcell_stride;
+      const int ncell = J.pcell_cnt[iprt];
+      float acc_psp = 0.0f;
+      for (int k = 32 * my_sub + lane; k < ncell; k += 32 * G) {
+        const int4 c = __ldg(cell + GD_AT(k, J.pcell_stride, kSitePsp));
+        const int p = GD_AT(c.x, P, kSitePos);
+        const float4 q = pos[p];
+        // -pmf0 of (t, point type): the pair table entry of the range's first atom
+        const int beg = c.y & 0xffff, end = c.y >> 16;
+        const int e = (beg >> 1) * kTabCols + __float_as_int(aux[p].y);
+        const float4 tb = apt[GD_AT(2 * e + 1, 2 * npairs * kTabCols, kSiteApt)];
+        const float thr = (beg & 1) ? tb.y : tb.x;
+        const float nx = -q.x, ny = -q.y, nz = -q.z;
+        int hits = 0;
+        for (int a = beg; a < end; ++a) {
+          const V4<float> la = atom_at(lp, GD_AT(a, L, kSiteLig));
+          const float dx = __fadd_rn(la.x, nx), dy = __fadd_rn(la.y, ny), dz = __fadd_rn(la.z, nz);
+          const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+          const float d = __fmul_rn(d2, rsqrt_approx(d2));
+          hits += __fadd_rn(d, thr) <= 0.0f ? 1 : 0;
+        }
+        acc_psp = fmaf((float)hits, __int_as_float(c.z), acc_psp);
+      }
+      s_psp += acc_psp;
     }
   } else {
     for (int row = row0; row < P; row += rstep) {

@@ -512,6 +512,38 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
       }
     }
 
+  // the same as non-zero cells per conformation for the ligand's types, by type then point
+  // (the batched kernel's pocket-specific pass), at a stride of the largest count or, with
+  // jd.cell_room, of every point times every type the ligand can have (a refill on the GPU
+  // of the same shapes always fits)
+  int tbeg[kLigTypes], tend[kLigTypes];
+  for (int t = 0; t < kLigTypes; ++t) tbeg[t] = tend[t] = 0;
+  for (int a = L - 1; a >= 0; --a) {
+    tbeg[ltype[a]] = a;
+    if (tend[ltype[a]] == 0) tend[ltype[a]] = a + 1;
+  }
+  std::vector<int> pcell_cnt(pk.nconf, 0);
+  for (int i = 0; i < pk.nconf; ++i)
+    for (int j = 0; j < P; ++j)
+      for (int t = 0; t < kLigTypes; ++t)
+        pcell_cnt[i] += (tend[t] > 0 && ((pspmask[(size_t)i * P + j] >> t) & 1u)) ? 1 : 0;
+  int cstride = jd.cell_room ? P * std::min(L, kLigTypes) : 1;
+  for (int i = 0; i < pk.nconf; ++i) cstride = std::max(cstride, pcell_cnt[i]);
+  std::vector<int4> pcell((size_t)pk.nconf * cstride, make_int4(0, 0, 0, 0));
+  for (int i = 0; i < pk.nconf; ++i) {
+    int k = 0;
+    for (int t = 0; t < kLigTypes; ++t) {
+      if (tend[t] == 0) continue;
+      for (int j = 0; j < P; ++j)
+        if ((pspmask[(size_t)i * P + j] >> t) & 1u) {
+          const float v = psp[((size_t)i * kLigTypes + t) * P + j];
+          int vb;
+          std::memcpy(&vb, &v, 4);
+          pcell[(size_t)i * cstride + k++] = make_int4(j, tbeg[t] | (tend[t] << 16), vb, t);
+        }
+    }
+  }
+
   DevParams par;
   GD_TRY(build_params(ep, jd.move_scale, par));
   std::vector<DevParams> parv(1, par);
@@ -535,6 +567,7 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   Arena ar;
   const size_t o_par = ar.put(parv), o_lig = ar.put(lig), o_lg = ar.put(lgrp), o_lc = ar.put(jd.lcenter);
   const size_t o_pm = ar.put(pspmask), o_hr = ar.put(ref4);
+  const size_t o_pc = ar.put(pcell), o_pcn = ar.put(pcell_cnt);
   const size_t o_kde = ar.put(kde), o_mcs = ar.put(mcs), o_tcc = ar.put(jd.tcc), o_psp = ar.put(psp);
   const size_t o_mb = ar.put(jd.minus_beta), o_rep = ar.put(jd.reps), o_acc = ar.put(run_acc), o_st = ar.put(stats);
   size_t o_rec = 0;
@@ -582,6 +615,9 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   J.pcenter = pk.center;
   J.psp = (const float *)(b + o_psp);
   J.pspmask = (const uint32_t *)(b + o_pm);
+  J.pcell = (const int4 *)(b + o_pc);
+  J.pcell_cnt = (const int *)(b + o_pcn);
+  J.pcell_stride = cstride;
   J.nkde = (int)kidx.size();
   J.kde = (const float4 *)(b + o_kde);
   for (int t = 0; t < kLigTypes; ++t) {

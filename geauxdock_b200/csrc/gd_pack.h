@@ -73,6 +73,7 @@ struct JobData {
   float move_scale[6] = {0, 0, 0, 0, 0, 0};
   uint64_t seed = 0;
   int nprt = 0;                      // protein conformations of the pocket
+  bool cell_room = false;            // pocket-specific cells: room for any potential of these shapes
   std::vector<ReplicaMC> reps;       // replicas to run (a contiguous range)
   int rid_base = 0;                  // ensemble index of reps[0]
   int nrep_total = 0;                // nlig * nprt * ntmp
@@ -142,6 +143,9 @@ struct PackDst {
   int *ncdc;
   float *psp;
   uint32_t *pspmask;
+  int4 *pcell;         // pocket-specific cells (nullptr: none; only the per-type-group form reads the job)
+  int *pcell_cnt;
+  int pcell_stride;    // cells per conformation the array holds
   int kde_cap;         // KDE points the kde array holds
   int Ppad;            // > 0: padded points per conformation the arrays hold (else from the Complex)
   int nkde_expect;     // >= 0: KDE points of ligand types the arrays hold
@@ -157,7 +161,7 @@ struct PackDst {
 };
 enum { kPackFailCapacity = 1, kPackFailInput = 2, kPackFailShape = 3 };
 enum { kFieldNLig = 1, kFieldNPrt, kFieldNatom, kFieldNatomConf, kFieldNpoint, kFieldKde, kFieldMcs, kFieldLigType,
-       kFieldPrtType, kFieldSeq3r, kFieldMcsRow, kFieldP1a, kFieldNTmp, kFieldReplica };
+       kFieldPrtType, kFieldSeq3r, kFieldMcsRow, kFieldP1a, kFieldNTmp, kFieldReplica, kFieldPcell };
 // Launches the packer on `st` (setup, pocket, ligand kernels); failures stay in D.err.
 cudaError_t device_pack(const Complex *d_cx, const PackDst &D, cudaStream_t st);
 const char *pack_field_name(int field);
