@@ -518,30 +518,39 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   // of the same shapes always fits)
   int tbeg[kLigTypes], tend[kLigTypes];
   for (int t = 0; t < kLigTypes; ++t) tbeg[t] = tend[t] = 0;
+  uint32_t ligmask = 0u;
   for (int a = L - 1; a >= 0; --a) {
     tbeg[ltype[a]] = a;
     if (tend[ltype[a]] == 0) tend[ltype[a]] = a + 1;
+    ligmask |= 1u << ltype[a];
   }
+  // per conformation: per-type counts, then each cell at its type's running offset
   std::vector<int> pcell_cnt(pk.nconf, 0);
+  std::vector<int> tcell((size_t)pk.nconf * kLigTypes, 0);
   for (int i = 0; i < pk.nconf; ++i)
     for (int j = 0; j < P; ++j)
-      for (int t = 0; t < kLigTypes; ++t)
-        pcell_cnt[i] += (tend[t] > 0 && ((pspmask[(size_t)i * P + j] >> t) & 1u)) ? 1 : 0;
+      for (uint32_t m = pspmask[(size_t)i * P + j] & ligmask; m; m &= m - 1u) ++tcell[(size_t)i * kLigTypes + __builtin_ctz(m)];
   int cstride = jd.cell_room ? P * std::min(L, kLigTypes) : 1;
-  for (int i = 0; i < pk.nconf; ++i) cstride = std::max(cstride, pcell_cnt[i]);
+  for (int i = 0; i < pk.nconf; ++i) {
+    for (int t = 0; t < kLigTypes; ++t) pcell_cnt[i] += tcell[(size_t)i * kLigTypes + t];
+    cstride = std::max(cstride, pcell_cnt[i]);
+  }
   std::vector<int4> pcell((size_t)pk.nconf * cstride, make_int4(0, 0, 0, 0));
   for (int i = 0; i < pk.nconf; ++i) {
-    int k = 0;
-    for (int t = 0; t < kLigTypes; ++t) {
-      if (tend[t] == 0) continue;
-      for (int j = 0; j < P; ++j)
-        if ((pspmask[(size_t)i * P + j] >> t) & 1u) {
-          const float v = psp[((size_t)i * kLigTypes + t) * P + j];
-          int vb;
-          std::memcpy(&vb, &v, 4);
-          pcell[(size_t)i * cstride + k++] = make_int4(j, tbeg[t] | (tend[t] << 16), vb, t);
-        }
+    int at[kLigTypes];
+    for (int t = 0, o = 0; t < kLigTypes; ++t) {
+      at[t] = o;
+      o += tcell[(size_t)i * kLigTypes + t];
     }
+    int4 *cell = pcell.data() + (size_t)i * cstride;
+    for (int j = 0; j < P; ++j)
+      for (uint32_t m = pspmask[(size_t)i * P + j] & ligmask; m; m &= m - 1u) {
+        const int t = __builtin_ctz(m);
+        const float v = psp[((size_t)i * kLigTypes + t) * P + j];
+        int vb;
+        std::memcpy(&vb, &v, 4);
+        cell[at[t]++] = make_int4(j, tbeg[t] | (tend[t] << 16), vb, t);
+      }
   }
 
   DevParams par;

@@ -271,6 +271,9 @@ def test_dock_reuses_device_state(lib, enepara):
             synth.make_job(rng, pka, 20, 2, 100, 5, temps, seed=2),
             synth.make_job(rng, pkb, 20, 2, 100, 5, temps, seed=3),
             synth.make_job(rng, pkb, 27, 3, 90, 4, temps, seed=4)]
+    # call 2's pocket-specific potential is non-zero everywhere: its refill holds
+    # more non-zero cells than the state was first packed with
+    jobs[1].psp = np.where(jobs[1].psp == 0, np.float32(-0.25), jobs[1].psp).astype(np.float32)
     pks = [pka, pka, pkb, pkb]
     cxs = [synth.to_complex(j, p, enepara, steps_total=100, steps_per_dump=50, steps_per_exchange=25)
            for j, p in zip(jobs, pks)]
