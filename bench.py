@@ -727,6 +727,12 @@ def run_ours(args) -> None:
             e2e_times.append(time.perf_counter() - t0)
     e2e_steps = int(cx[0]["mcpara"]["steps_total"])
     e2e_s = sum(e2e_times)
+    # device-to-host bytes of a call: the Record entries the kernels wrote straight into the
+    # pinned array as the chunk ran (with their next_entry words), or, on the copy path, the
+    # whole Record array; then the final replica states
+    rec_direct = bool(lib.gd_get_option(b"dock_record_direct"))
+    rec_bytes = (int(rec_h["next_entry"].astype(np.int64).sum()) * Lo.REPLICA.itemsize + 4 * n_rep if rec_direct
+                 else Lo.RECORD.itemsize * n_rep)
     if world > 1:                        # the slowest rank's time, as for the device-timed value
         t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -754,8 +760,10 @@ def run_ours(args) -> None:
             "config": _config(n_rep, world),
             "autotune": tune.strip().splitlines()[-1] if tune else "off",
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": Lo.COMPLEX.itemsize,
-                    "d2h_bytes_per_step": Lo.RECORD.itemsize * n_rep + Lo.REPLICA.itemsize * n_rep,
-                    "step": f"one Dock call: CopyH2D + initial energies + {e2e_steps} MC steps + Record copy",
+                    "d2h_bytes_per_step": rec_bytes + Lo.REPLICA.itemsize * n_rep,
+                    "step": f"one Dock call: CopyH2D + initial energies + {e2e_steps} MC steps + Records to the "
+                            "pinned host array" + (" (written by the kernels as the steps run)" if rec_direct
+                                                   else " (copied after the chunk)"),
                     "calls": e2e_calls, "call_ms": [round(1e3 * t, 2) for t in e2e_times],
                     "timing": "host wall clock around each call (synchronised), summed; max over ranks"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",

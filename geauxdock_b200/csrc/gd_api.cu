@@ -21,12 +21,13 @@ struct Options {
   int kernel = GD_KERNEL_BATCHED;
   int precision = GD_PREC_FP32_KAHAN;  // FP32 pair terms, compensated reductions
   int warps = 0;  // 0: choose from occupancy
-  int kpl = 2;
-  int ab = 8;
+  int kpl = 0;    // pair-tile shape, 0: default_pair_tile
+  int ab = 0;
   int graph = 1;  // replay whole exchange intervals from a captured graph
   int stage = -1; // protein conformation in shared memory: 1 staged, 0 through L1, -1 chosen
   int dock_cache = 1;  // Dock keeps its device state per GPU between calls
   int dock_device_pack = 1;  // Dock refills that state on the GPU from the Complex CopyH2D put there
+  int dock_record_direct = 1;  // Dock's kernels write Records straight into a GPU-mapped host array
   int replica_warps = 1;     // warps per replica (1, 2, 4, 8): latency mode of the batched FP32 kernel
   int device_base = 0;        // the drop-in API's GPU g is CUDA device device_base + g
   long long wait_limit = 0;   // microseconds of a bounded shared-memory wait (0: one second)
@@ -304,6 +305,7 @@ int finish_create(gd_ensemble *e)
   e->wait_limit = (uint32_t)o.wait_limit;
   e->stall_bytes = o.stall_test ? 16u : 0u;
   TileConfig tc{o.warps > 0 ? o.warps : 8, o.kpl, o.ab, o.stage != 0 ? 1 : 0, o.replica_warps};
+  default_pair_tile(tc.group, tc.kpl, tc.ab);
   if (e->precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8, tc.group = 1;
   if (o.warps > 0) return configure(e, tc);
   return choose_warps(e, tc, o.stage);
@@ -724,10 +726,10 @@ int gd_set_option(const char *name, long long v)
     if (v < 0 || v > kMaxCtaThreads / 32) return fail(GD_E_INVALID, "warps = %lld", v);
     g_opt.warps = (int)v;
   } else if (n == "kpl") {
-    if (v != 1 && v != 2 && v != 4) return fail(GD_E_INVALID, "kpl = %lld", v);
+    if (v != 0 && v != 1 && v != 2 && v != 4) return fail(GD_E_INVALID, "kpl = %lld", v);
     g_opt.kpl = (int)v;
   } else if (n == "ab") {
-    if (v != 4 && v != 8) return fail(GD_E_INVALID, "ab = %lld", v);
+    if (v != 0 && v != 4 && v != 8) return fail(GD_E_INVALID, "ab = %lld", v);
     g_opt.ab = (int)v;
   } else if (n == "stage") {
     if (v < -1 || v > 1) return fail(GD_E_INVALID, "stage = %lld", v);
@@ -741,6 +743,9 @@ int gd_set_option(const char *name, long long v)
   } else if (n == "dock_device_pack") {
     if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_device_pack = %lld", v);
     g_opt.dock_device_pack = (int)v;
+  } else if (n == "dock_record_direct") {
+    if (v != 0 && v != 1) return fail(GD_E_INVALID, "dock_record_direct = %lld", v);
+    g_opt.dock_record_direct = (int)v;
   } else if (n == "device_base") {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess) count = 0;
@@ -778,6 +783,7 @@ long long gd_get_option(const char *name)
   if (n == "stage") return g_opt.stage;
   if (n == "replica_warps") return g_opt.replica_warps;
   if (n == "dock_device_pack") return g_opt.dock_device_pack;
+  if (n == "dock_record_direct") return g_opt.dock_record_direct;
   if (n == "dock_cache") return g_opt.dock_cache;
   if (n == "wait_limit") return g_opt.wait_limit;
   if (n == "device_base") return g_opt.device_base;
@@ -954,6 +960,13 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
     return fail(GD_E_INVALID, "steps_per_dump = %d outside [1, %d] (Record capacity)", spd, GD_STEPS_PER_DUMP);
   const int spx = (mp.steps_per_exchange > 0 && ch->size.n_tmp > 1) ? mp.steps_per_exchange : 0;
   std::vector<gd_ensemble *> ens(n, nullptr);
+  // where the kernels write the Records: the device array rd[g], copied to rh after each
+  // chunk (backend_gpu.cu:108-110), or, when rh is page-locked host memory this GPU can
+  // address (cudaHostAlloc, or cudaHostRegister with mapping), rh itself: each entry then
+  // crosses PCIe as the kernel writes it, while the chunk runs, and no copy follows
+  std::vector<Record *> rdst(n, nullptr);
+  std::vector<char> direct(n, 0);
+  const bool try_direct = opts().dock_record_direct != 0;
   int rc = GD_OK;
   Tracer tr("Dock");
   for (int g = 0; g < n && rc == GD_OK; ++g) {
@@ -961,9 +974,21 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
       rc = fail(GD_E_STATE, "Dock before DeviceAlloc/InitCurand on GPU %d", g);
       break;
     }
+    rdst[g] = rd[g];
+    if (try_direct && (rc = set_device(dev_of(g))) == GD_OK) {
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, rh + pt[g]->rep_begin) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+          at.devicePointer != nullptr) {
+        rdst[g] = (Record *)at.devicePointer;
+        direct[g] = 1;
+      } else {
+        (void)cudaGetLastError();  // pageable memory: the copy below
+      }
+    }
+    if (rc != GD_OK) break;
     // each Dock call draws a fresh stream from the handle (the reference's curand state advances)
     const uint64_t seed = rng[g]->seed + (rng[g]->calls++ << 32);
-    rc = dock_ensemble(rng[g], ch, cd[g], pt[g]->rep_begin, pt[g]->rep_end, seed, rd[g], dev_of(g), &ens[g]);
+    rc = dock_ensemble(rng[g], ch, cd[g], pt[g]->rep_begin, pt[g]->rep_end, seed, rdst[g], dev_of(g), &ens[g]);
   }
   tr.mark("pack+create");
   // initial energy, backend_gpu.cu:87-91: one step, no move, forced accept
@@ -982,8 +1007,10 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
     for (int g = 0; g < n && rc == GD_OK; ++g) {
       rc = set_device(dev_of(g));
       if (rc != GD_OK) break;
-      const cudaError_t ce = cudaMemcpyAsync(rh + pt[g]->rep_begin, rd[g], sizeof(Record) * (size_t)pt[g]->n_rep,
-                                             cudaMemcpyDeviceToHost, ens[g]->st);
+      const cudaError_t ce =
+          direct[g] ? cudaSuccess
+                    : cudaMemcpyAsync(rh + pt[g]->rep_begin, rd[g], sizeof(Record) * (size_t)pt[g]->n_rep,
+                                      cudaMemcpyDeviceToHost, ens[g]->st);
       if (ce == cudaSuccess) {
         const cudaError_t se = cudaStreamSynchronize(ens[g]->st);
         if (se != cudaSuccess) rc = fail(GD_E_CUDA, "Dock: %s", cudaGetErrorString(se));
@@ -1032,6 +1059,7 @@ int eval_on(gd_ensemble *e, int job, int n, const int *conf, const float *mm, in
       return fail(GD_E_INVALID, "pose %d: conformation (%d, %d) out of range", i, conf[2 * i], conf[2 * i + 1]);
   const Options o = opts();
   TileConfig tc{8, o.kpl, o.ab};
+  default_pair_tile(1, tc.kpl, tc.ab);
   if (precision == GD_PREC_FP64) tc.kpl = 1, tc.ab = 8;
   int kst = precision == GD_PREC_FP64 ? J.nkde : 0;  // FP32: KDE points through L1
   int P = e->Pmax;

@@ -553,6 +553,7 @@ int server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *e
   s->tc.group = s->cfg.replica_warps > 0 ? s->cfg.replica_warps : 1;
   if (s->tc.group != 1 && s->tc.group != 2 && s->tc.group != 4 && s->tc.group != 8)
     return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8)", s->cfg.replica_warps);
+  default_pair_tile(s->tc.group, s->tc.kpl, s->tc.ab);
   if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1;
   if (s->tc.kpl % 2) s->tc.group = 1;  // the split form exists for the FP32 atom-pair loop
   GD_TRY(server_configure(s));

@@ -94,14 +94,23 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
 
 /* Options: "kernel" (GD_KERNEL_*), "precision" (GD_PREC_*, default
  * GD_PREC_FP32_KAHAN), "warps" (replicas
- * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape; default 2, 8),
+ * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape: pocket points per
+ * lane 1, 2 or 4, atoms per hydrophobic block 4 or 8; default 0, the
+ * library's choice: 4, 4 with one warp per replica, 2, 8 in latency mode),
  * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
  * 0: launch them one by one), "stage" (1: stage each protein conformation in
  * shared memory, 0: read it through L1, -1: choose by occupancy; pockets too
  * large to stage are always read through L1), "dock_cache" (1: Dock keeps
  * its packed device state per GPU handle and refills it in place when the next
  * Complex has the same shapes, keeping the packed protein when its bytes are
- * unchanged; 0: everything is rebuilt and freed per call), "device_base" (the
+ * unchanged; 0: everything is rebuilt and freed per call), "dock_device_pack"
+ * (1: that refill packs the Complex CopyH2D put on the GPU, on the GPU; 0: the
+ * host re-packs it), "dock_record_direct" (1: when Dock's Record array rh is
+ * page-locked host memory the GPU can address -- cudaHostAlloc, or
+ * cudaHostRegister with mapping -- the kernels write each Record entry into it
+ * as the chunk runs and no copy follows; entries at and past a Record's
+ * next_entry keep what rh held; 0, or pageable rh: the Records go to rd[g] and
+ * the whole array is copied to rh after each chunk), "device_base" (the
  * drop-in API's GPU g is CUDA device device_base + g, for one process per GPU;
  * set it before SetDevice/DeviceAlloc and keep it), "wait_limit"
  * (microseconds, on the GPU's global timer, that the kernel's bounded

@@ -80,7 +80,7 @@ def main() -> None:
                     violations.append({"shape": si, "tile": tile, "precision": prec, "site": SITES[r[1]],
                                        "index": r[2], "length": r[3]})
     check(lib.gd_set_option(b"precision", GD_PREC_FP32_KAHAN))
-    for k, v in (("warps", 0), ("kpl", 2), ("ab", 8), ("stage", -1)):
+    for k, v in (("warps", 0), ("kpl", 0), ("ab", 0), ("stage", -1)):
         check(lib.gd_set_option(k.encode(), v))
     print(json.dumps({"cases": cases, "violations": violations, "raced": raced, "max_scaled_error": worst}))
 

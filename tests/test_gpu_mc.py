@@ -309,6 +309,49 @@ def test_dock_reuses_device_state(lib, enepara):
         assert a == b == c
 
 
+def test_dock_records_direct_to_pinned_host(lib, enepara):
+    """With a page-locked Record array the kernels write the Records straight
+    into it (option dock_record_direct): the replica states and every Record's
+    entries below next_entry equal those of the copy path, and the entries past
+    next_entry keep what the array held (nothing is copied over them)."""
+    import torch
+
+    rng = np.random.default_rng(23)
+    pk = synth.make_pocket(rng, 300, 2)
+    temps = np.array([0.3, 0.9, 2.7], np.float32)
+    # one dump chunk: every entry this call writes is below next_entry (with more chunks,
+    # entries an earlier chunk wrote past the last chunk's count stay, on both paths)
+    cx = synth.to_complex(synth.make_job(rng, pk, 20, 2, 100, 5, temps, seed=3), pk, enepara,
+                          steps_total=60, steps_per_dump=60, steps_per_exchange=20)
+    n = int(cx[0]["size"]["n_rep"])
+
+    def written(w, rec):
+        reps = w[0]["replica"][:n]
+        fields = tuple(reps[f].tobytes() for f in reps.dtype.names)
+        entries = tuple(rec[r]["replica"][:int(rec[r]["next_entry"])].tobytes() for r in range(n))
+        return fields, entries, rec["next_entry"][:n].tobytes()
+
+    out = {}
+    for mode, direct in (("copy", 0), ("direct", 1)):
+        check(lib.gd_set_option(b"dock_record_direct", direct))
+        try:
+            buf = torch.full((Lo.RECORD.itemsize * n,), 0xAB, dtype=torch.uint8, pin_memory=True)
+            rec = np.frombuffer(buf.numpy(), dtype=Lo.RECORD, count=n)
+            with dock.DockSession(1, seed=9) as s:
+                w = cx.copy()
+                s.dock(w, rec)
+                out[mode] = written(w, rec)
+                ne = rec["next_entry"][:n].copy()
+                assert (ne >= 1).all() and (ne <= 61).all()       # the initial state and the accepted moves
+                tail = [rec[r]["replica"][int(ne[r]):].tobytes() for r in range(n)]
+                untouched = all(t == b"\xab" * len(t) for t in tail)
+                # the copy path overwrites the whole array with the device one
+                assert untouched == bool(direct), mode
+        finally:
+            check(lib.gd_set_option(b"dock_record_direct", 1))
+    assert out["copy"] == out["direct"]
+
+
 def test_dock_device_refill_refuses_invalid(lib, enepara):
     """A Complex the device packer refuses on a refill (a ligand atom type out of
     range) fails the Dock call with GD_E_INVALID before any kernel reads it; the

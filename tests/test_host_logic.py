@@ -64,10 +64,10 @@ def test_options_validated(lib):
         check(lib.gd_set_option(b"kernel", 7))
     with pytest.raises(GdockError):
         check(lib.gd_set_option(b"nonsense", 1))
-    assert lib.gd_get_option(b"kpl") == 2          # default pair-tile shape
+    assert lib.gd_get_option(b"kpl") == 0          # default pair-tile shape: the library's choice
     check(lib.gd_set_option(b"kpl", 4))
     assert lib.gd_get_option(b"kpl") == 4
-    check(lib.gd_set_option(b"kpl", 2))
+    check(lib.gd_set_option(b"kpl", 0))
     assert lib.gd_get_option(b"graph") == 1
     assert lib.gd_get_option(b"stage") == -1
     assert lib.gd_get_option(b"dock_cache") == 1
