@@ -1437,7 +1437,7 @@ int gd_ensemble_autotune(gd_ensemble_t *e, int steps, char *report, int report_l
   std::string rep;
   TileConfig best = e->tc;
   double best_t = 1e300;
-  const int shapes[][2] = {{1, 8}, {2, 4}, {2, 8}, {4, 4}};
+  const int shapes[][2] = {{1, 8}, {2, 4}, {2, 8}, {4, 4}, {4, 8}};
   const int warps[] = {4, 6, 8, 10, 12, 14, 16};
   const bool can_stage = smem_for(e, std::max(4, e->tc.group), 0, 1, e->tc.group) <= kSmemLimit;
   cudaEvent_t a, b;

@@ -180,15 +180,16 @@ struct TileConfig {
 };
 
 // Pair-tile shape where the caller leaves it to the library (option value 0):
-// 4 points per lane and 4-atom hydrophobic blocks with one warp per replica;
-// 2 and 8 in latency mode, whose warps share a replica's rows (shorter rows
-// deal out more evenly).  Measured on the batched FP32 kernel: 4 x 4 runs the
-// 3520-replica ensemble 1.2 % and a one-replica 600-point complex 9 % faster
-// than 2 x 8, and a replica on 4 or 8 warps 14-25 % slower.
+// 4 points per lane with one warp per replica, 2 in latency mode, whose warps
+// share a replica's rows (shorter rows deal out more evenly); 8-atom
+// hydrophobic blocks.  Measured on the batched FP32 kernel: 4 x 8 runs the
+// 3520-replica Dock call 1.8 % and a one-replica 600-point complex 10 %
+// faster than 2 x 8, and 4 points per lane make a replica on 4 or 8 warps
+// 14-25 % slower.
 inline void default_pair_tile(int group, int &kpl, int &ab)
 {
   if (kpl == 0) kpl = group > 1 ? 2 : 4;
-  if (ab == 0) ab = group > 1 ? 8 : 4;
+  if (ab == 0) ab = 8;
 }
 
 enum Precision { kFP32 = 0, kFP32Kahan = 1, kFP64 = 2 };

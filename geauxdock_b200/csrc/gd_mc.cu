@@ -1356,6 +1356,7 @@ static cudaError_t launch_p(const KArgs &a, const TileConfig &tc, int grid, cuda
   if (tc.kpl == 2 && tc.ab == 4) return launch_t<MODE, PREC, 2, 4>(a, w, grid, st);
   if (tc.kpl == 2 && tc.ab == 8) return launch_t<MODE, PREC, 2, 8>(a, w, grid, st);
   if (tc.kpl == 4 && tc.ab == 4) return launch_t<MODE, PREC, 4, 4>(a, w, grid, st);
+  if (tc.kpl == 4 && tc.ab == 8) return launch_t<MODE, PREC, 4, 8>(a, w, grid, st);
   return cudaErrorInvalidValue;
 }
 
@@ -1381,7 +1382,8 @@ int kernel_occupancy(int mode, int precision, const TileConfig &tc, size_t smem)
   if (mode == M && precision == PR && tc.kpl == K && tc.ab == A)                              \
     f = split ? (const void *)mc_kernel<M, PR, K, A, (M == 0 && PR != kFP64 && K % 2 == 0)> \
               : (const void *)mc_kernel<M, PR, K, A, false>;
-#define GD_PICK_ALL(M, PR) GD_PICK(M, PR, 1, 8) GD_PICK(M, PR, 2, 4) GD_PICK(M, PR, 2, 8) GD_PICK(M, PR, 4, 4)
+#define GD_PICK_ALL(M, PR) \
+  GD_PICK(M, PR, 1, 8) GD_PICK(M, PR, 2, 4) GD_PICK(M, PR, 2, 8) GD_PICK(M, PR, 4, 4) GD_PICK(M, PR, 4, 8)
   GD_PICK_ALL(0, kFP32) GD_PICK_ALL(0, kFP32Kahan) GD_PICK_ALL(0, kFP64)
   GD_PICK_ALL(1, kFP32) GD_PICK_ALL(1, kFP32Kahan) GD_PICK_ALL(1, kFP64)
 #undef GD_PICK_ALL

@@ -96,7 +96,7 @@ int Dock(Complex *ch, Record *rh, Complex **cd, Record **rd, ParaT **pt, gd_rng_
  * GD_PREC_FP32_KAHAN), "warps" (replicas
  * per CTA, 0 = autotune), "kpl", "ab" (pair-tile shape: pocket points per
  * lane 1, 2 or 4, atoms per hydrophobic block 4 or 8; default 0, the
- * library's choice: 4, 4 with one warp per replica, 2, 8 in latency mode),
+ * library's choice: 4, 8 with one warp per replica, 2, 8 in latency mode),
  * "graph" (1: replay whole exchange intervals from a captured CUDA graph,
  * 0: launch them one by one), "stage" (1: stage each protein conformation in
  * shared memory, 0: read it through L1, -1: choose by occupancy; pockets too

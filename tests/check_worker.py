@@ -43,7 +43,7 @@ def main() -> None:
     rng = np.random.default_rng(5)
     shapes = [(8, 64, 12, 2, 2, 2, (0.3, 0.9, 2.7)), (7, 37, 9, 1, 1, 2, (0.5, 1.5)), (1, 1, 0, 1, 1, 1, (1.0,)),
               (5, 64, 6, 3, 3, 1, (0.4,)), (8, 63, 20, 4, 1, 3, (0.3, 0.6, 1.2, 2.4))]
-    tiles = [(1, 2, 8, 0), (3, 2, 8, 0), (3, 2, 8, 1), (2, 2, 4, 1), (4, 4, 4, 0), (2, 1, 8, 0)]
+    tiles = [(1, 2, 8, 0), (3, 2, 8, 0), (3, 2, 8, 1), (2, 2, 4, 1), (4, 4, 4, 0), (2, 4, 8, 1), (2, 1, 8, 0)]
     violations, worst, cases, raced = [], 0.0, 0, []
     report(lib)
     for si, (L, P, K, M, nlig, nprt, temps) in enumerate(shapes):
