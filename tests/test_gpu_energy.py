@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from geauxdock_b200 import dock, synth
-from geauxdock_b200._lib import GD_PREC_FP32, GD_PREC_FP32_KAHAN, GD_PREC_FP64
+from geauxdock_b200._lib import GD_PREC_FP32, GD_PREC_FP32_KAHAN, GD_PREC_FP64, check
 from oracle import tolerance as TOL
 
 pytestmark = pytest.mark.gpu
@@ -91,6 +91,45 @@ def test_edge_sizes(lib, enepara, oracle_lib):
         conf = np.zeros((12, 2), np.int32)
         out, _, _ = dock.eval_poses(cx, conf, mm, GD_PREC_FP32)
         _check(out, _oracle_energies(oracle_lib, cx, conf, mm), f"L={L} P={P}")
+
+
+@pytest.mark.parametrize("kind", ["none", "dense", "other_types"])
+@pytest.mark.parametrize("kpl", [2, 4])
+def test_pocket_specific_cells(lib, enepara, oracle_lib, kind, kpl):
+    """The pocket-specific term walked over the potential's non-zero cells: no
+    cell at all, every (class-2 point, ligand type) cell, and cells only for
+    types the ligand does not have (none of them walked), at 2 and 4 points per
+    lane; close contacts (poses near the cavity centre) so that d <= pmf0 holds
+    for many pairs."""
+    rng = np.random.default_rng(11)
+    pk = synth.make_pocket(rng, 400, 2)
+    job = synth.make_job(rng, pk, 17, 2, 120, 4, [1.0], seed=5)
+    present = np.zeros(24, bool)
+    present[np.unique(job.lig_type)] = True
+    if kind == "none":
+        job.psp = np.zeros_like(job.psp)
+    elif kind == "dense":
+        job.psp = rng.uniform(-1.0, -0.1, size=job.psp.shape).astype(np.float32)
+    else:
+        job.psp = np.where(present[:, None], 0.0, rng.uniform(-1.0, -0.1, size=job.psp.shape)).astype(np.float32)
+    cx = synth.to_complex(job, pk, enepara)
+    n = 24
+    mm = synth.config4_poses(kpl + 40, n, radius=2.0)
+    conf = np.stack([np.arange(n) % 2, (np.arange(n) // 2) % 2], axis=1).astype(np.int32)
+    res = [oracle_lib.energy(cx, int(c[0]), int(c[1]), m) for c, m in zip(conf, mm)]
+    ref = np.array([r[0] for r in res])
+    ref_raw = np.array([r[1] for r in res])
+    check(lib.gd_set_option(b"kpl", kpl))
+    try:
+        out, raw, _ = dock.eval_poses(cx, conf, mm, GD_PREC_FP32_KAHAN)
+    finally:
+        check(lib.gd_set_option(b"kpl", 0))
+    # raw term 3: the pocket-specific sum before normalisation
+    if kind != "dense":
+        assert np.all(ref_raw[:, 3] == 0.0) and np.all(raw[:, 3] == 0.0)
+    else:
+        assert np.count_nonzero(ref_raw[:, 3]) > n // 2
+    _check(out, ref, f"psp {kind}, kpl {kpl}")
 
 
 @pytest.mark.parametrize("L", [127, 128])
