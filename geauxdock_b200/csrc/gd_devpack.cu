@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restri
   }
   __syncthreads();
   if (warp < kLigTypes && s_tcnt[warp] > 0) {
-    int4 *cell = D.pcell + (size_t)i * D.pcell_stride;
+    int4 *cell = D.pcell + (size_t)i * D.pcell_stride * 2;
     const int t = warp, rng = s_tbeg[t] | ((s_tbeg[t] + s_tcnt[t]) << 16);
     int at = s_cbeg[t];
     for (int j0 = 0; j0 < Pp; j0 += 32) {
@@ -386,7 +386,13 @@ __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restri
       const bool m = j < Pp && ((pm[j] >> t) & 1u);
       const unsigned b = __ballot_sync(0xffffffffu, m);
       const int o = at + __popc(b & ((1u << lane) - 1u));
-      if (m && o < D.pcell_stride) cell[o] = make_int4(j, rng, __float_as_int(psp[(size_t)t * Pp + j]), t);
+      if (m && o < D.pcell_stride) {
+        const float4 q = pos[j];
+        const int pt = __float_as_int(aux[j].y);
+        cell[2 * o] = make_int4(__float_as_int(q.x), __float_as_int(q.y), __float_as_int(q.z),
+                                __float_as_int(psp[(size_t)t * Pp + j]));
+        cell[2 * o + 1] = make_int4(rng, __float_as_int(D.par->tab4[t][pt].z), t, j);
+      }
       at += __popc(b);
     }
   }

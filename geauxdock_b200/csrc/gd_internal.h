@@ -122,11 +122,12 @@ struct DevJob {
   const uint32_t *pspmask; // [nprt][npoint_pad] bit t set where psp[.][t][p] != 0
   // the same potential as a list of its non-zero cells (sorted point p, ligand type t) per
   // conformation, for the types the ligand has, ordered by type, then point: cell k <
-  // pcell_cnt[c] of conformation c is pcell[c * pcell_stride + k] = (p, beg | end << 16,
-  // bits of the value, t), [beg, end) the atoms of type t in the type-grouped ligand
+  // pcell_cnt[c] of conformation c is the int4 pair pcell[2 (c * pcell_stride + k) + {0, 1}] =
+  // (bits of x, y, z of point p and of the value), (beg | end << 16, bits of -pmf0 of (t, type
+  // of p), t, p), [beg, end) the atoms of type t in the type-grouped ligand
   const int4 *pcell;
   const int *pcell_cnt;    // [nprt]
-  int pcell_stride;
+  int pcell_stride;        // cells per conformation
   // KDE
   int nkde;
   const float4 *kde;       // [nkde]

@@ -541,23 +541,21 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     // non-zero cells (point p, ligand type t, value v; only types the ligand
     // has), ordered by type: lane k takes cell k and counts the atoms of type t
     // (the contiguous range [beg, end) of the type-grouped ligand) with
-    // d - pmf0 <= 0.  d, -pmf0 (from the same pair table) and the comparison are
-    // the pair loop's operations in the same order, so an atom counts here
-    // exactly where that loop would count it.
+    // d - pmf0 <= 0.  d, -pmf0 (the value the pair tables hold) and the
+    // comparison are the pair loop's operations in the same order, so an atom
+    // counts here exactly where that loop would count it.
     {
-      const int4 *cell = J.pcell + (size_t)iprt * J.pcell_stride;
+      const int4 *cell = J.pcell + (size_t)iprt * J.pcell_stride * 2;
       const int ncell = J.pcell_cnt[iprt];
       float acc_psp = 0.0f;
       for (int k = 32 * my_sub + lane; k < ncell; k += 32 * G) {
-        const int4 c = __ldg(cell + GD_AT(k, J.pcell_stride, kSitePsp));
-        const int p = GD_AT(c.x, P, kSitePos);
-        const float4 q = pos[p];
-        // -pmf0 of (t, point type): the pair table entry of the range's first atom
-        const int beg = c.y & 0xffff, end = c.y >> 16;
-        const int e = (beg >> 1) * kTabCols + __float_as_int(aux[p].y);
-        const float4 tb = apt[GD_AT(2 * e + 1, 2 * npairs * kTabCols, kSiteApt)];
-        const float thr = (beg & 1) ? tb.y : tb.x;
-        const float nx = -q.x, ny = -q.y, nz = -q.z;
+        // the point's coordinates and value, and the atom range with -pmf0 of
+        // (t, point type), the pair table's value: two independent 16-byte loads
+        const int4 c0 = __ldg(cell + 2 * GD_AT(k, J.pcell_stride, kSitePsp));
+        const int4 c1 = __ldg(cell + 2 * k + 1);
+        const int beg = c1.x & 0xffff, end = c1.x >> 16;
+        const float thr = __int_as_float(c1.y);
+        const float nx = -__int_as_float(c0.x), ny = -__int_as_float(c0.y), nz = -__int_as_float(c0.z);
         int hits = 0;
         for (int a = beg; a < end; ++a) {
           const V4<float> la = atom_at(lp, GD_AT(a, L, kSiteLig));
@@ -566,7 +564,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           const float d = __fmul_rn(d2, rsqrt_approx(d2));
           hits += __fadd_rn(d, thr) <= 0.0f ? 1 : 0;
         }
-        acc_psp = fmaf((float)hits, __int_as_float(c.z), acc_psp);
+        acc_psp = fmaf((float)hits, __int_as_float(c0.w), acc_psp);
       }
       s_psp += acc_psp;
     }

@@ -55,6 +55,12 @@ inline float as_float(int i)
   std::memcpy(&f, &i, 4);
   return f;
 }
+inline int as_int(float f)
+{
+  int i;
+  std::memcpy(&i, &f, 4);
+  return i;
+}
 }  // namespace
 
 namespace {
@@ -381,6 +387,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cu
   std::vector<int> ncdc(n, 0);
   out.scls.assign((size_t)n * Ppad, -1);
   out.sseq.assign((size_t)n * Ppad, 0);
+  out.stype.assign((size_t)n * Ppad, kPadType);
   for (int i = 0; i < n; ++i) {
     const int np = pk.npts[i];
     std::vector<int> idx(np);
@@ -408,6 +415,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cu
         aux[o] = make_float2(pk.cdc[s] == 1 ? pk.hpp[s] : 0.f, as_float(pk.type[s]));
         out.scls[o] = pk.cls[s];
         out.sseq[o] = pk.seq3r[s];
+        out.stype[o] = pk.type[s];
       } else {
         // inert padding: far away, zero parameters, point type kPadType (all-zero table column)
         pos[o] = make_float4(1.0e4f + (float)j, 1.0e4f, 1.0e4f, 0.f);
@@ -415,6 +423,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cu
       }
     }
   }
+  out.spos = pos;
   Arena ar;
   const size_t o_pos = ar.put(pos), o_aux = ar.put(aux), o_c = ar.put(pk.center), o_n = ar.put(ncdc);
   if (reuse && reuse->arena && reuse->bytes == ar.off) {
@@ -512,10 +521,14 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
       }
     }
 
+  DevParams par;
+  GD_TRY(build_params(ep, jd.move_scale, par));
+
   // the same as non-zero cells per conformation for the ligand's types, by type then point
-  // (the batched kernel's pocket-specific pass), at a stride of the largest count or, with
-  // jd.cell_room, of every point times every type the ligand can have (a refill on the GPU
-  // of the same shapes always fits)
+  // (the batched kernel's pocket-specific pass), two int4 per cell: (x, y, z of the point,
+  // value) and (beg | end << 16, -pmf0 of (type, point type), type, point), at a stride of
+  // the largest count or, with jd.cell_room, of every point times every type the ligand can
+  // have (a refill on the GPU of the same shapes always fits)
   int tbeg[kLigTypes], tend[kLigTypes];
   for (int t = 0; t < kLigTypes; ++t) tbeg[t] = tend[t] = 0;
   uint32_t ligmask = 0u;
@@ -535,26 +548,26 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
     for (int t = 0; t < kLigTypes; ++t) pcell_cnt[i] += tcell[(size_t)i * kLigTypes + t];
     cstride = std::max(cstride, pcell_cnt[i]);
   }
-  std::vector<int4> pcell((size_t)pk.nconf * cstride, make_int4(0, 0, 0, 0));
+  std::vector<int4> pcell((size_t)pk.nconf * cstride * 2, make_int4(0, 0, 0, 0));
   for (int i = 0; i < pk.nconf; ++i) {
     int at[kLigTypes];
     for (int t = 0, o = 0; t < kLigTypes; ++t) {
       at[t] = o;
       o += tcell[(size_t)i * kLigTypes + t];
     }
-    int4 *cell = pcell.data() + (size_t)i * cstride;
+    int4 *cell = pcell.data() + (size_t)i * cstride * 2;
     for (int j = 0; j < P; ++j)
       for (uint32_t m = pspmask[(size_t)i * P + j] & ligmask; m; m &= m - 1u) {
         const int t = __builtin_ctz(m);
+        const size_t o = (size_t)i * P + j;
+        const float4 q = pk.spos[o];
         const float v = psp[((size_t)i * kLigTypes + t) * P + j];
-        int vb;
-        std::memcpy(&vb, &v, 4);
-        cell[at[t]++] = make_int4(j, tbeg[t] | (tend[t] << 16), vb, t);
+        const int k = at[t]++;
+        cell[2 * k] = make_int4(as_int(q.x), as_int(q.y), as_int(q.z), as_int(v));
+        cell[2 * k + 1] = make_int4(tbeg[t] | (tend[t] << 16), as_int(par.tab4[t][pk.stype[o]].z), t, j);
       }
   }
 
-  DevParams par;
-  GD_TRY(build_params(ep, jd.move_scale, par));
   std::vector<DevParams> parv(1, par);
   std::vector<float4> ref4((size_t)kLigTypes * kTabCols, make_float4(0.f, 0.f, 0.f, 0.f));
   for (int lt = 0; lt < kLigTypes; ++lt)

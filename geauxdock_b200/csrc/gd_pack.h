@@ -87,6 +87,8 @@ struct DevPocket {
   float *center = nullptr;           // [nconf][3]
   int *ncdc = nullptr;               // [nconf] hydrophobic-contact points (placed first)
   std::vector<int> scls, sseq;       // host: class and residue serial of each sorted point
+  std::vector<float4> spos;          // host: pos of each sorted point
+  std::vector<int> stype;            // host: point type of each sorted point (kPadType for padding)
   void *arena = nullptr;
   size_t bytes = 0;
 };
