@@ -651,8 +651,9 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
 
   // Pass 2: hydrophobic contact (energy_prt_v1.cu:42-49) over the rows that
   // hold cdc == 1 points (placed first).  The polynomial
-  // 1 - 3.5x + 4.5x^2 - 2.5x^3 + 0.5x^4 (x = d^2/81) is (1-x)^3 (1-x/2);
-  // clamping 1-x at 0 applies the d^2 <= 81 cut-off.  Per-atom sums stay in
+  // 1 - 3.5x + 4.5x^2 - 2.5x^3 + 0.5x^4 (x = d^2/81) is (1-x)^3 (1-x/2), i.e.
+  // (y^3 + y^4) / 2 with y = 1 - x; clamping y at 0 applies the d^2 <= 81
+  // cut-off.  Per-atom sums stay in
   // registers for AB atoms at a time, then the per-atom restraint
   // (energy_prt_v1.cu:162-169).
   T ehpc = 0;
@@ -662,8 +663,9 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       T hpc[AB];
       if constexpr (PREC != kFP64 && KPL % 2 == 0) {
         // atom-pair form, the same operations per component: h2[k] holds the
-        // sums of atoms a0 + 2k and a0 + 2k + 1 (AB is even)
-        const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f), c2 = f2(-0.5f / 81.0f);
+        // sums of atoms a0 + 2k and a0 + 2k + 1 (AB is even) of hpp (y^2 (y + y^2)),
+        // twice the contact sum (halved exactly at the end)
+        const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f);
         float2 h2[AB / 2];
 #pragma unroll
         for (int k = 0; k < AB / 2; ++k) h2[k] = f2(0.0f);
@@ -687,19 +689,19 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
             for (int j = 0; j < KPL; ++j) {
               const float2 dx = __fadd2_rn(la.x, npx[j]), dy = __fadd2_rn(la.y, npy[j]), dz = __fadd2_rn(la.z, npz[j]);
               const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-              float2 t = __ffma2_rn(d2, c1, one);
-              t.x = fmaxf(t.x, 0.0f);
-              t.y = fmaxf(t.y, 0.0f);
-              const float2 u = __ffma2_rn(d2, c2, one);
-              const float2 w = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, t), t), u);
+              float2 y = __ffma2_rn(d2, c1, one);
+              y.x = fmaxf(y.x, 0.0f);
+              y.y = fmaxf(y.y, 0.0f);
+              const float2 yy = __fmul2_rn(y, y);
+              const float2 w = __fmul2_rn(yy, __fadd2_rn(y, yy));
               h2[k] = __ffma2_rn(ph2[j], w, h2[k]);
             }
           }
         }
 #pragma unroll
         for (int k = 0; k < AB / 2; ++k) {
-          hpc[2 * k] = h2[k].x;
-          hpc[2 * k + 1] = h2[k].y;
+          hpc[2 * k] = 0.5f * h2[k].x;
+          hpc[2 * k + 1] = 0.5f * h2[k].y;
         }
       } else {
 #pragma unroll
