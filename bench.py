@@ -55,14 +55,14 @@ STEPS_PER_INTERVAL = 50
 # DRAM bytes (read + write) of one Monte Carlo launch of this workload (3520
 # replicas x 50 steps, tile 8 x kpl 4 x ab 8, pocket read through L1): a RECORDED
 # constant, not measured by this script.  From one capture on a B200 of the kernel
-# of commit 6ea4611 (profiles/mc_kernel_ensemble3520_traffic.md):
+# of commit 2316429 (profiles/mc_kernel_ensemble3520_traffic.md):
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:mc_kernel -s 4 -c 1
 #       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,4,8,0
-# (1,700,864 B read + 51,712 B written); it does not grow with the steps per launch.
-TRAFFIC_BYTES_PER_LAUNCH = 1_700_864 + 51_712
+# (1,845,248 B read + 116,736 B written); it does not grow with the steps per launch.
+TRAFFIC_BYTES_PER_LAUNCH = 1_845_248 + 116_736
 TRAFFIC_SOURCE = ("recorded constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
-                  "kernel of commit 6ea4611, profiles/mc_kernel_ensemble3520_traffic.md")
+                  "kernel of commit 2316429, profiles/mc_kernel_ensemble3520_traffic.md")
 
 
 def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
