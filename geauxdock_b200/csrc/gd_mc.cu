@@ -292,7 +292,6 @@ template <int KPL>
 struct PairAccP {
   float2 vdw, pmf, hdb;
   float2 ele[KPL];
-  float psp;
 };
 
 // Per work item, shared-memory tables of the atom-pair pair loop, built from
@@ -330,19 +329,18 @@ __device__ void build_pair_tables(int L, const DevParams *par, const int2 *lg, f
 // (energy_prt_v1.cu:56-139 except the hydrophobic contact), the FP32 forms of
 // pair_atoms with two atoms per packed f32x2 instruction (__ffma2_rn /
 // __fadd2_rn / __fmul2_rn, sm_100); the special functions stay per component.
-// HDB / PSP: evaluate the hydrogen-bond / pocket-specific terms (some point of
-// the row has a parameter for one of the two atoms).  npx/npy/npz hold the
-// lane's negated point coordinates twice (x_atom - x_point is x_atom + (-x_point),
-// exactly); the charges and, for PSP, the two atom types are read from shared
-// memory where they are used, which keeps the loop within its registers.
-template <int KPL, bool HDB, bool PSP>
+// HDB: evaluate the hydrogen-bond term (some point of the row has a parameter
+// for one of the two atoms); the pocket-specific term is walked over its
+// non-zero cells after the loop.  npx/npy/npz hold the lane's negated point
+// coordinates twice (x_atom - x_point is x_atom + (-x_point), exactly); the
+// charges are read from shared memory where they are used, which keeps the
+// loop within its registers.
+template <int KPL, bool HDB>
 __device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, int i GD_CHECK_ARG(int npairs), const float2 &lx,
                                                const float2 &ly, const float2 &lz, const float4 *__restrict__ apt,
-                                               const float4 *__restrict__ aph, const int4 *__restrict__ ahd,
-                                               const int (&pt)[KPL], const uint32_t (&pm)[KPL],
+                                               const float4 *__restrict__ aph, const int (&pt)[KPL],
                                                const float2 (&npx)[KPL], const float2 (&npy)[KPL],
-                                               const float2 (&npz)[KPL], const float *__restrict__ pspc, int P,
-                                               int row, int lane, const PairConst &c, PairAccP<KPL> &acc)
+                                               const float2 (&npz)[KPL], const PairConst &c, PairAccP<KPL> &acc)
 {
   const float2 lj01 = f2(c.lj01), lj0 = f2(c.lj0), one = f2(1.0f), inv_el1 = f2(c.inv_el1);
   const float2 za = f2(-0.5f * kLog2e), zb = f2(6.0f * kLog2e);
@@ -367,12 +365,6 @@ __device__ __forceinline__ void pair_atom_pair(const LigPair *__restrict__ lig, 
     const float2 z = __fmul2_rn(__ffma2_rn(za, d, zb), dmp);
     const float2 e1 = __fadd2_rn(make_float2(ex2_approx(z.x), ex2_approx(z.y)), one);
     acc.pmf = __ffma2_rn(make_float2(tb.z, tb.w), make_float2(rcp_approx(e1.x), rcp_approx(e1.y)), acc.pmf);
-    if constexpr (PSP) {
-      const int p = row + 32 * j + lane;
-      const int lta = ahd[GD_AT(i, npairs, kSiteAhd)].z, ltb = ahd[i].w;
-      if (((pm[j] >> lta) & 1u) && dmp.x <= 0.0f) acc.psp += __ldg(pspc + GD_AT((size_t)lta * P + p, kLigTypes * P, kSitePsp));
-      if (((pm[j] >> ltb) & 1u) && dmp.y <= 0.0f) acc.psp += __ldg(pspc + GD_AT((size_t)ltb * P + p, kLigTypes * P, kSitePsp));
-    }
     if constexpr (HDB) {
       const float4 th = aph[GD_AT(e, npairs * kTabCols, kSiteAph)];
       const float2 h = __ffma2_rn(d, make_float2(th.x, th.y), make_float2(th.z, th.w));
@@ -484,7 +476,6 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
     for (int row = row0; row < P; row += rstep) {
       float2 npx[KPL], npy[KPL], npz[KPL];
       int pt[KPL];
-      uint32_t pm[KPL];
       uint32_t ptbits = 0u;
 #pragma unroll
       for (int j = 0; j < KPL; ++j) {
@@ -494,7 +485,6 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         npy[j] = f2(-q.y);
         npz[j] = f2(-q.z);
         pt[j] = __float_as_int(aux[p].y);
-        pm[j] = 0u;
         ptbits |= 1u << pt[j];
       }
       // point types present in the row: decide per atom pair, for the whole
@@ -504,16 +494,15 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
       acc.vdw = acc.pmf = acc.hdb = f2(0.0f);
 #pragma unroll
       for (int j = 0; j < KPL; ++j) acc.ele[j] = f2(0.0f);
-      acc.psp = 0.0f;
       for (int i = 0; i < npairs; ++i) {
         const int2 fl = *reinterpret_cast<const int2 *>(&ahd[GD_AT(i, npairs, kSiteAhd)].x);
         const bool any_hdb = ((uint32_t)fl.x & ptbits) != 0u;
         const float4 l01 = *reinterpret_cast<const float4 *>(&lp[GD_AT(i, npairs, kSiteLig)].x);
         const float2 lx = make_float2(l01.x, l01.y), ly = make_float2(l01.z, l01.w), lz = lp[i].z;
         if (any_hdb)
-          pair_atom_pair<KPL, true, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+          pair_atom_pair<KPL, true>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, pt, npx, npy, npz, kc, acc);
         else
-          pair_atom_pair<KPL, false, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, ahd, pt, pm, npx, npy, npz, pspc, P, row, lane, kc, acc);
+          pair_atom_pair<KPL, false>(lp, i GD_CHECK_ARG(npairs), lx, ly, lz, apt, aph, pt, npx, npy, npz, kc, acc);
       }
       float row_ele = 0.f;
 #pragma unroll
@@ -527,13 +516,11 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         kahan_add(s_vdw, c_vdw, row_vdw);
         kahan_add(s_ele, c_ele, row_ele);
         kahan_add(s_pmf, c_pmf, row_pmf);
-        s_psp += acc.psp;
         s_hdb += row_hdb;
       } else {
         s_vdw += row_vdw;
         s_ele += row_ele;
         s_pmf += row_pmf;
-        s_psp += acc.psp;
         s_hdb += row_hdb;
       }
     }
