@@ -632,8 +632,9 @@ int dock_ensemble(gd_rng *h, const Complex *c, const Complex *d_cx, int rb, int 
     GD_TRY(job_from_complex(c, rb, re, seed, jd));
     jd.cell_room = true;  // the arena keeps the size of the one it refills
     bool ok = true;
-    const bool same_prt =
-        h->dock_prt.size() == prt_bytes && std::memcmp(h->dock_prt.data(), c->prt, prt_bytes) == 0;
+    const bool same_prt = h->dock_prt.size() == prt_bytes &&
+                          std::memcmp(h->dock_prt.data(), c->prt, prt_bytes) == 0 &&
+                          e->pockets[0].hdb_types == hdb_point_types(c->enepara);
     if (!same_prt) {
       PocketData pk;
       GD_TRY(pocket_from_complex(c, pk));
@@ -1212,6 +1213,7 @@ int gd_ensemble_create(const gd_pocket_desc_t *pockets, int npocket, const gd_jo
   for (int p = 0; p < npocket && rc == GD_OK; ++p) {
     PocketData pk;
     rc = pocket_from_desc(pockets[p], pk);
+    pk.hdb_types = hdb_point_types(*enepara);
     if (rc == GD_OK) rc = pack_pocket(pk, e->pockets[p]);
     nconf[p] = pockets[p].nconf;
   }
@@ -1260,7 +1262,7 @@ int gd_ensemble_create_complex(const Complex *const *cx, int n, const uint64_t *
     for (size_t q = 0; q < seen.size(); ++q)
       if (seen[q].nconf == pk.nconf && seen[q].npts == pk.npts && seen[q].xyz == pk.xyz && seen[q].type == pk.type &&
           seen[q].cls == pk.cls && seen[q].cdc == pk.cdc && seen[q].seq3r == pk.seq3r && seen[q].hpp == pk.hpp &&
-          seen[q].ele == pk.ele && seen[q].center == pk.center) {
+          seen[q].ele == pk.ele && seen[q].center == pk.center && seen[q].hdb_types == pk.hdb_types) {
         p = (int)q;
         break;
       }

@@ -7,8 +7,9 @@
 // with the same orders, so that both packings of one Complex are identical
 // byte for byte:
 //   - ligand atoms grouped by type, stable (util_optimize_soa.C:112-126);
-//   - pocket points with the hydrophobic-contact flag first, each part sorted
-//     by point type, stable, padded with inert points (type 30, far away);
+//   - pocket points with the hydrophobic-contact flag first; in each part the
+//     point types with a hydrogen-bond parameter first, each group sorted by
+//     point type, stable; padded with inert points (type 30, far away);
 //   - KDE points of ligand types sorted by type, stable, with per-type ranges
 //     (util_optimize_soa.C:336-372; points of other types cannot match);
 //   - MCS templates atom-major in grouped order, validity as energy_mcs_v1.cu;
@@ -273,7 +274,7 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
 }
 
 // One CTA per protein conformation: points ordered as the host packer orders
-// them (hydrophobic-contact points first, each part sorted by point type,
+// them (hydrophobic-contact points first, each part by hydrogen-bond group and point type,
 // stable; 60 buckets (cdc, type), two per warp, counted and scattered with
 // warp ballots), inert padding, the pocket-specific potential gathered with
 // its non-zero type mask, and its non-zero cells for the ligand's types, by
@@ -281,7 +282,7 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
 __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restrict__ cx, PackDst D)
 {
   constexpr int kBuckets = 2 * kPadType;
-  __shared__ int s_cnt[kBuckets], s_beg[kBuckets];
+  __shared__ int s_cnt[kBuckets], s_beg[kBuckets], s_rank[kPadType];
   if (*(volatile int *)D.err & kErrPack) return;
   const int i = blockIdx.x;
   const int nprt = cx->size.n_prt;
@@ -292,7 +293,21 @@ __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restri
   const int np = pr.prt_npoint;
   const int Pp = D.Ppad > 0 ? D.Ppad : ((P + kPointAlign - 1) / kPointAlign) * kPointAlign;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  auto bucket = [&](int k) { return (pr.cdc[k] == 1 ? 0 : kPadType) + pr.t[k]; };
+  // the host packer's order: per part (cdc == 1 first) the point types with a
+  // hydrogen-bond parameter first, each group by type: rank of each type
+  if (threadIdx.x == 0) {
+    uint32_t m = 0;
+    for (int lt = 0; lt < kLigTypes; ++lt)
+      for (int pt = 0; pt < kPadType; ++pt)
+        if (cx->enepara.hdb0[lt][pt] > 0.1f) m |= 1u << pt;
+    int r = 0;
+    for (int pt = 0; pt < kPadType; ++pt)
+      if ((m >> pt) & 1u) s_rank[pt] = r++;
+    for (int pt = 0; pt < kPadType; ++pt)
+      if (!((m >> pt) & 1u)) s_rank[pt] = r++;
+  }
+  __syncthreads();
+  auto bucket = [&](int k) { return (pr.cdc[k] == 1 ? 0 : kPadType) + s_rank[pr.t[k]]; };
   for (int bk = warp; bk < kBuckets; bk += nwarps) {
     int cnt = 0;
     for (int k0 = 0; k0 < np; k0 += 32) {

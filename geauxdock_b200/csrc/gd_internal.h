@@ -9,6 +9,7 @@
 //
 //   pocket conformation  pos[P] float4 (x, y, z, ele), aux[P] float2 (hpp_eff,
 //                        type): hydrophobic-contact points first, each part
+//                        with the hydrogen-bond point types first, each group
 //                        sorted by point type, padded with inert points
 //   force-field tables   tab4[24][32] float4 (1/p1a, -p2a/p1a, -pmf0, pmf1) for the FP32 pair loop
 //                        tab2[24][32] float2 (hdb1 c, -hdb0 hdb1 c), zero where hdb0 <= 0.1

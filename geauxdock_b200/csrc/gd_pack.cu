@@ -143,6 +143,7 @@ int pocket_from_complex(const Complex *c, PocketData &pk)
   pk = PocketData{};
   pk.nconf = nprt;
   pk.P = P;
+  pk.hdb_types = hdb_point_types(c->enepara);
   pk.npts.resize(nprt);
   pk.xyz.assign((size_t)nprt * P * 3, 0.f);
   pk.type.assign((size_t)nprt * P, 0);
@@ -327,6 +328,15 @@ int job_from_desc(const gd_job_desc_t &d, int nprt, JobData &jd)
   return GD_OK;
 }
 
+uint32_t hdb_point_types(const EnePara &ep)
+{
+  uint32_t m = 0;
+  for (int lt = 0; lt < kLigTypes; ++lt)
+    for (int pt = 0; pt < kPadType; ++pt)
+      if (ep.hdb0[lt][pt] > 0.1f) m |= 1u << pt;
+  return m;
+}
+
 int build_params(const EnePara &ep, const float move_scale[6], DevParams &p)
 {
   std::memset(&p, 0, sizeof(p));
@@ -382,6 +392,7 @@ int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cu
   const int Ppad = ((std::max(pk.P, 1) + kPointAlign - 1) / kPointAlign) * kPointAlign;
   out.nconf = n;
   out.Ppad = Ppad;
+  out.hdb_types = pk.hdb_types;
   std::vector<float4> pos((size_t)n * Ppad);
   std::vector<float2> aux((size_t)n * Ppad);
   std::vector<int> ncdc(n, 0);
@@ -397,10 +408,13 @@ int pack_pocket(const PocketData &pk, DevPocket &out, const DevPocket *reuse, cu
       if (t < 0 || t >= kPadType) return fail(GD_E_INVALID, "protein conformation %d point %d: type %d outside [0, %d)", i, k, t, kPadType);
     }
     // hydrophobic-contact points first (their rows are the only ones the
-    // hydrophobic term visits), each part sorted by point type
+    // hydrophobic term visits); in each part the point types with a
+    // hydrogen-bond parameter first (the pair loop evaluates that term only for
+    // rows holding such a type), each group sorted by point type
     auto key = [&](int k) {
       const size_t o = (size_t)i * pk.P + k;
-      return (pk.cdc[o] == 1 ? 0 : 64) + pk.type[o];
+      const int t = pk.type[o];
+      return (pk.cdc[o] == 1 ? 0 : 64) + (((pk.hdb_types >> t) & 1u) ? 0 : 32) + t;
     };
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
     int nc = 0;

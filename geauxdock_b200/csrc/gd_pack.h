@@ -51,7 +51,12 @@ struct PocketData {
   std::vector<int> type, cls, cdc, seq3r;  // [nconf][P]
   std::vector<float> hpp, ele;       // [nconf][P]
   std::vector<float> center;         // [nconf][3]
+  uint32_t hdb_types = 0;            // point types with a hydrogen-bond parameter (sorted first in each part)
 };
+
+// Point types with a hydrogen-bond parameter for some ligand type (hdb0 > 0.1,
+// the reference's guard): bit pt.
+uint32_t hdb_point_types(const EnePara &ep);
 
 // One docking job in dense host arrays.
 struct JobData {
@@ -89,6 +94,7 @@ struct DevPocket {
   std::vector<int> scls, sseq;       // host: class and residue serial of each sorted point
   std::vector<float4> spos;          // host: pos of each sorted point
   std::vector<int> stype;            // host: point type of each sorted point (kPadType for padding)
+  uint32_t hdb_types = 0;            // the PocketData::hdb_types it was sorted with
   void *arena = nullptr;
   size_t bytes = 0;
 };

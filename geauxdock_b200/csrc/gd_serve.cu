@@ -541,6 +541,7 @@ int server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *e
   for (int i = 0; i < npocket; ++i) {
     PocketData pd;
     GD_TRY(pocket_from_desc(pockets[i], pd));
+    pd.hdb_types = hdb_point_types(s->ep);
     DevPocket dp;
     GD_TRY(pack_pocket(pd, dp));
     s->pockets.push_back(dp);
