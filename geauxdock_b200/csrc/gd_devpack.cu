@@ -6,7 +6,8 @@
 // OptimizeMcs / OptimizeEnepara, src/frontend/util_optimize_soa.C:37-540),
 // with the same orders, so that both packings of one Complex are identical
 // byte for byte:
-//   - ligand atoms grouped by type, stable (util_optimize_soa.C:112-126);
+//   - ligand atoms grouped by type, stable (util_optimize_soa.C:112-126), the
+//     types with a hydrogen-bond parameter first;
 //   - pocket points with the hydrophobic-contact flag first; in each part the
 //     point types with a hydrogen-bond parameter first, each group sorted by
 //     point type, stable; padded with inert points (type 30, far away);
@@ -35,17 +36,37 @@ __device__ void dp_fail(const PackDst &D, int kind, int field, int value)
 
 __device__ __forceinline__ float dp_as_float(int i) { return __int_as_float(i); }
 
-// Ligand atoms grouped by type (stable): perm[k] = input index of grouped atom k.
+// The host packer's order of the ligand type groups: the types with a
+// hydrogen-bond parameter for some point type first, each part by type.
+__device__ void dp_ligand_type_order(const Complex *cx, int *order)
+{
+  uint32_t m = 0;
+  for (int lt = 0; lt < kLigTypes; ++lt)
+    for (int pt = 0; pt < kPadType; ++pt)
+      if (cx->enepara.hdb0[lt][pt] > 0.1f) m |= 1u << lt;
+  int q = 0;
+  for (int t = 0; t < kLigTypes; ++t)
+    if ((m >> t) & 1u) order[q++] = t;
+  for (int t = 0; t < kLigTypes; ++t)
+    if (!((m >> t) & 1u)) order[q++] = t;
+}
+
+// Ligand atoms grouped by type in that order (stable): perm[k] = input index
+// of grouped atom k.
 __device__ void dp_ligand_order(const Complex *cx, int L, int *perm, int *ltype)
 {
+  int order[kLigTypes];
+  dp_ligand_type_order(cx, order);
   int k = 0;
-  for (int t = 0; t < kLigTypes; ++t)
+  for (int q = 0; q < kLigTypes; ++q) {
+    const int t = order[q];
     for (int a = 0; a < L; ++a)
       if (cx->lig[0].t2[a] == t) {
         perm[k] = a;
         ltype[k] = t;
         ++k;
       }
+  }
 }
 
 // Sizes, validation, force-field tables, ligand atom order, KDE points sorted
@@ -381,11 +402,16 @@ __global__ void __launch_bounds__(1024) dp_pocket_kernel(const Complex *__restri
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // atom ranges in the grouped ligand's type order, cells by type index
+    int order[kLigTypes];
+    dp_ligand_type_order(cx, order);
     int a = 0, c = 0;
+    for (int q = 0; q < kLigTypes; ++q) {
+      s_tbeg[order[q]] = a;
+      a += s_tcnt[order[q]];
+    }
     for (int t = 0; t < kLigTypes; ++t) {
-      s_tbeg[t] = a;
       s_cbeg[t] = c;
-      a += s_tcnt[t];
       c += s_ccnt[t];
     }
     D.pcell_cnt[i] = min(c, D.pcell_stride);

@@ -469,10 +469,17 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
     if (jd.ltype[a] < 0 || jd.ltype[a] >= kLigTypes)
       return fail(GD_E_INVALID, "ligand atom %d: type %d outside [0, %d)", a, jd.ltype[a], kLigTypes);
 
-  // atoms grouped by type (stable), the order of the reference's sorted copy (util_optimize_soa.C:112-126)
+  // atoms grouped by type (stable), as the reference's sorted copy (util_optimize_soa.C:112-126),
+  // with the types that have a hydrogen-bond parameter first (an atom pair of the pair loop then
+  // mixes such a type with one without at most once)
+  uint32_t lhdb = 0;
+  for (int lt = 0; lt < kLigTypes; ++lt)
+    for (int pt = 0; pt < kPadType; ++pt)
+      if (ep.hdb0[lt][pt] > 0.1f) lhdb |= 1u << lt;
+  auto lkey = [&](int t) { return (((lhdb >> t) & 1u) ? 0 : 32) + t; };
   std::vector<int> perm(L);
   std::iota(perm.begin(), perm.end(), 0);
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return jd.ltype[a] < jd.ltype[b]; });
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return lkey(jd.ltype[a]) < lkey(jd.ltype[b]); });
   const int lstride = (L + 3) & ~3;
   std::vector<float4> lig((size_t)jd.nlig * lstride, make_float4(0, 0, 0, 0));
   for (int i = 0; i < jd.nlig; ++i)
