@@ -43,7 +43,9 @@ def main() -> None:
     rng = np.random.default_rng(5)
     shapes = [(8, 64, 12, 2, 2, 2, (0.3, 0.9, 2.7)), (7, 37, 9, 1, 1, 2, (0.5, 1.5)), (1, 1, 0, 1, 1, 1, (1.0,)),
               (5, 64, 6, 3, 3, 1, (0.4,)), (8, 63, 20, 4, 1, 3, (0.3, 0.6, 1.2, 2.4))]
-    tiles = [(1, 2, 8, 0), (3, 2, 8, 0), (3, 2, 8, 1), (2, 2, 4, 1), (4, 4, 4, 0), (2, 4, 8, 1), (2, 1, 8, 0)]
+    # (warps per CTA, kpl, ab, stage[, warps per replica: latency mode])
+    tiles = [(1, 2, 8, 0), (3, 2, 8, 0), (3, 2, 8, 1), (2, 2, 4, 1), (4, 4, 4, 0), (2, 4, 8, 1), (2, 1, 8, 0),
+             (4, 2, 8, 0, 2), (8, 2, 8, 1, 4), (8, 4, 8, 0, 8)]
     violations, worst, cases, raced = [], 0.0, 0, []
     report(lib)
     for si, (L, P, K, M, nlig, nprt, temps) in enumerate(shapes):
@@ -56,10 +58,11 @@ def main() -> None:
         e64 = np.array([O.energy(cx, int(c[0]), int(c[1]), m)[0] for c, m in zip(conf, mm)])
         runs = {}
         for tile in tiles:
-            for k, v in zip(("warps", "kpl", "ab", "stage"), tile):
+            g = tile[4] if len(tile) > 4 else 1
+            for k, v in zip(("warps", "kpl", "ab", "stage", "replica_warps"), (*tile[:4], g)):
                 check(lib.gd_set_option(k.encode(), v))
             for prec in (GD_PREC_FP32, GD_PREC_FP32_KAHAN, GD_PREC_FP64):
-                if prec == GD_PREC_FP64 and tile[1] != 1:
+                if prec == GD_PREC_FP64 and (tile[1] != 1 or g > 1):
                     continue
                 check(lib.gd_set_option(b"precision", prec))
                 with dock.Ensemble.from_complexes([cx], [7]) as ens:
@@ -70,7 +73,7 @@ def main() -> None:
                     ens.sync()
                     reps = ens.replicas(0)
                 cases += 1
-                key = (tile[1], tile[2], prec)
+                key = (tile[1], tile[2], prec, g)
                 b = reps.tobytes()
                 if key in runs and runs[key] != b:
                     raced.append({"shape": si, "tile": tile, "precision": prec})
@@ -80,7 +83,7 @@ def main() -> None:
                     violations.append({"shape": si, "tile": tile, "precision": prec, "site": SITES[r[1]],
                                        "index": r[2], "length": r[3]})
     check(lib.gd_set_option(b"precision", GD_PREC_FP32_KAHAN))
-    for k, v in (("warps", 0), ("kpl", 0), ("ab", 0), ("stage", -1)):
+    for k, v in (("warps", 0), ("kpl", 0), ("ab", 0), ("stage", -1), ("replica_warps", 1)):
         check(lib.gd_set_option(k.encode(), v))
     print(json.dumps({"cases": cases, "violations": violations, "raced": raced, "max_scaled_error": worst}))
 
