@@ -81,7 +81,7 @@ class ServerStats(C.Structure):
         ("launches", C.c_longlong), ("pose_evals", C.c_double), ("device_ms", C.c_double), ("now", C.c_double),
         ("used_bytes", C.c_ulonglong), ("peak_bytes", C.c_ulonglong),
         ("warps_per_cta", C.c_int), ("grid", C.c_int), ("max_active_replicas", C.c_int),
-        ("pocket_staged", C.c_int),
+        ("pocket_staged", C.c_int), ("latency_rounds", C.c_longlong),
     ]
 
 

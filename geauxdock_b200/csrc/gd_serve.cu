@@ -85,6 +85,11 @@ struct gd_server {
   int precision = GD_PREC_FP32;
   int grid = 0, Pmax = 0, Kst = 0, lig_slots = 0;
   size_t smem = 0;
+  // adaptive latency mode (replica_warps < 0): the latency-mode launch shape,
+  // and the replica-warps one wave of it holds
+  TileConfig tcl{8, 2, 8};
+  int grid_l = 0, Kst_l = 0;
+  long long wave_l = 0;
   int max_items = 0;
   // device tables
   DevJob *d_jobs = nullptr;
@@ -210,9 +215,9 @@ void complete(gd_server *s, std::vector<ServeReq *> &done)
 
 // Items of one launch: runs of consecutive replicas with the same protein
 // conformation, at most warps_per_cta long, heaviest job first.
-void append_items(const gd_server *s, const ServeReq &r, std::vector<WorkItem> &out)
+void append_items(const TileConfig &tc, const ServeReq &r, std::vector<WorkItem> &out)
 {
-  const int R = s->tc.warps_per_cta / s->tc.group;  // replicas per CTA
+  const int R = tc.warps_per_cta / tc.group;  // replicas per CTA
   const std::vector<ReplicaMC> &reps = r.jd.reps;
   int i = 0;
   while (i < r.nrep) {
@@ -234,6 +239,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   const int R = s->cfg.steps_per_round;
   int nmax = 0, nslot = 0, max_pairs = 0;
   bool any_fresh = false;
+  long long nrep_act = 0;
   for (ServeReq *r : act) {
     int n = std::min(R, r->steps - r->step);
     if (r->spx > 0) n = std::min(n, r->spx - r->step % r->spx);
@@ -241,7 +247,13 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
     nmax = std::max(nmax, n);
     nslot = std::max(nslot, r->slot + 1);
     any_fresh |= r->fresh;
+    nrep_act += r->nrep;
   }
+  // adaptive latency mode: a round whose replicas, each on tcl.group warps,
+  // fit one wave of the grid runs in latency mode
+  const bool lat = s->tcl.group > 1 && nrep_act <= s->wave_l;
+  const TileConfig &tc = lat ? s->tcl : s->tc;
+  const int grid = lat ? s->grid_l : s->grid;
   // job table of this round
   DevJob *hj = s->h_jobs[b];
   for (int i = 0; i < nslot; ++i) hj[i] = DevJob{};
@@ -262,8 +274,8 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   });
   std::vector<WorkItem> items, init;
   for (ServeReq *r : ord) {
-    if (r->nstep_round > 0) append_items(s, *r, items);
-    if (r->fresh) append_items(s, *r, init);
+    if (r->nstep_round > 0) append_items(tc, *r, items);
+    if (r->fresh) append_items(tc, *r, init);
   }
   const int n_chunk = (int)items.size(), n_init = (int)init.size();
   if (n_chunk + n_init > s->max_items) return fail(GD_E_CAPACITY, "round of %d work items", n_chunk + n_init);
@@ -277,10 +289,10 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   a.jobs = s->d_jobs;
   a.queue = s->d_queue;
   a.err = s->d_err;
-  a.P = s->tc.stage ? s->Pmax : 0;
-  a.Kst = s->Kst;
+  a.P = tc.stage ? s->Pmax : 0;
+  a.Kst = lat ? s->Kst_l : s->Kst;
   a.lig_slots = s->lig_slots;
-  a.group = (uint16_t)s->tc.group;
+  a.group = (uint16_t)tc.group;
   int launches = 0;
   GD_CUDA(cudaEventRecord(s->t_ev[b][0], s->st));
   if (any_fresh) {
@@ -290,7 +302,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
     a.nsteps = 1;
     a.flags = kMcInitial | kMcStoreAccept;
     GD_CUDA(cudaMemsetAsync(s->d_queue, 0, sizeof(int), s->st));
-    GD_CUDA(launch_kernel(0, s->precision, s->tc, a, std::max(1, std::min(s->grid, n_init)), s->st));
+    GD_CUDA(launch_kernel(0, s->precision, tc, a, std::max(1, std::min(grid, n_init)), s->st));
     ++launches;
   }
   if (n_chunk > 0) {
@@ -300,7 +312,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
     a.nsteps = nmax;
     a.flags = kMcStoreAccept;
     GD_CUDA(cudaMemsetAsync(s->d_queue, 0, sizeof(int), s->st));
-    GD_CUDA(launch_kernel(0, s->precision, s->tc, a, std::max(1, std::min(s->grid, n_chunk)), s->st));
+    GD_CUDA(launch_kernel(0, s->precision, tc, a, std::max(1, std::min(grid, n_chunk)), s->st));
     ++launches;
   }
   if (max_pairs > 0) {
@@ -329,6 +341,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stats.rounds += 1;
+    s->stats.latency_rounds += lat ? 1 : 0;
     s->stats.launches += launches;
     s->stats.pose_evals += evals;
     for (ServeReq *r : finishing) s->active_reps -= r->nrep;
@@ -461,11 +474,13 @@ void serve_loop(gd_server *s)
   fail_all(s, GD_E_CANCELLED);
 }
 
-int server_configure(gd_server *s)
+// Launch shape of tile tc's group: warps per CTA and pocket staging from the
+// resident replica-warps per SM; sets tc, grid, Kst, smem and the CTAs per SM.
+int choose_shape(gd_server *s, TileConfig &tc_out, int &grid, int &Kst, size_t &smem_out, int &occ_out)
 {
   int nsm = 0;
   GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device));
-  const int G = s->tc.group;
+  const int G = tc_out.group;
   const int w0 = s->cfg.warps, wlo = w0 > 0 ? w0 : std::max(2, G), whi = w0 > 0 ? w0 : kMaxCtaThreads / 32;
   int best_w = 0, best_res = 0, best_occ = 0, best_kst = 0, best_stage = 1;
   size_t best_smem = 0;
@@ -474,7 +489,7 @@ int server_configure(gd_server *s)
   for (int stage = 1; stage >= 0; --stage)
   for (int w = wlo; w <= whi; ++w) {
     if (w % G) continue;
-    TileConfig tc = s->tc;
+    TileConfig tc = tc_out;
     tc.warps_per_cta = w;
     tc.stage = stage;
     const int P = stage ? s->Pmax : 0;
@@ -498,14 +513,29 @@ int server_configure(gd_server *s)
     }
   }
   if (best_w == 0) return fail(GD_E_CAPACITY, "no launch shape fits shared memory");
-  s->tc.warps_per_cta = best_w;
-  s->tc.stage = best_stage;
-  s->Kst = best_kst;
-  s->smem = best_smem;
-  s->grid = best_occ * nsm;
+  tc_out.warps_per_cta = best_w;
+  tc_out.stage = best_stage;
+  Kst = best_kst;
+  smem_out = best_smem;
+  grid = best_occ * nsm;
+  occ_out = best_occ;
+  return GD_OK;
+}
+
+int server_configure(gd_server *s)
+{
+  int occ = 0;
+  GD_TRY(choose_shape(s, s->tc, s->grid, s->Kst, s->smem, occ));
   // four waves of resident replica-warps per round: more balanced rounds (items
   // of uneven jobs) than two, with the same latency below saturation
-  if (s->cfg.max_active_replicas <= 0) s->cfg.max_active_replicas = 4 * best_occ * nsm * (best_w / G);
+  if (s->cfg.max_active_replicas <= 0)
+    s->cfg.max_active_replicas = 4 * s->grid * (s->tc.warps_per_cta / s->tc.group);
+  if (s->tcl.group > 1) {
+    size_t smem_l = 0;
+    int occ_l = 0;
+    GD_TRY(choose_shape(s, s->tcl, s->grid_l, s->Kst_l, smem_l, occ_l));
+    s->wave_l = (long long)s->grid_l * (s->tcl.warps_per_cta / s->tcl.group);
+  }
   return GD_OK;
 }
 
@@ -551,12 +581,20 @@ int server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *e
   const long long o_kpl = gd_get_option("kpl"), o_ab = gd_get_option("ab");
   s->precision = (int)gd_get_option("precision");
   s->tc = TileConfig{8, (int)o_kpl, (int)o_ab};
-  s->tc.group = s->cfg.replica_warps > 0 ? s->cfg.replica_warps : 1;
+  const int rw = s->cfg.replica_warps;
+  const int adapt = rw < 0 ? -rw : 0;
+  s->tc.group = rw > 0 ? rw : 1;
   if (s->tc.group != 1 && s->tc.group != 2 && s->tc.group != 4 && s->tc.group != 8)
-    return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8)", s->cfg.replica_warps);
+    return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8; -2, -4 or -8: adaptive)", rw);
+  if (adapt && adapt != 2 && adapt != 4 && adapt != 8)
+    return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8; -2, -4 or -8: adaptive)", rw);
+  s->tcl = TileConfig{8, (int)o_kpl, (int)o_ab};
+  s->tcl.group = adapt;
   default_pair_tile(s->tc.group, s->tc.kpl, s->tc.ab);
-  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1;
+  default_pair_tile(std::max(adapt, 2), s->tcl.kpl, s->tcl.ab);
+  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1, s->tcl.group = 0;
   if (s->tc.kpl % 2) s->tc.group = 1;  // the split form exists for the FP32 atom-pair loop
+  if (s->tcl.kpl % 2) s->tcl.group = 0;
   GD_TRY(server_configure(s));
   s->max_items = s->cfg.max_active_replicas * 2 + s->cfg.max_replicas_per_job;
   GD_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));

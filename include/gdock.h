@@ -305,7 +305,11 @@ typedef struct gd_server_config {
   int warps;                /* warps per CTA, 0: occupancy model */
   int device;
   int replica_warps;        /* warps per replica, 1 (default), 2, 4 or 8: latency mode, every
-                               replica's pair rows and KDE points split over that many warps */
+                               replica's pair rows and KDE points split over that many warps;
+                               -2, -4 or -8: adaptive, a round whose active replicas times that
+                               many warps fit the grid's resident warps runs in latency mode,
+                               others one warp per replica (a request's results then depend on
+                               the load it met, within the parity tolerance either way) */
 } gd_server_config_t;
 
 typedef struct gd_request {
@@ -332,6 +336,7 @@ typedef struct gd_server_stats {
   unsigned long long used_bytes, peak_bytes;
   int warps_per_cta, grid, max_active_replicas;
   int pocket_staged;                /* 1: pockets staged in shared memory, 0: read through L1 */
+  long long latency_rounds;         /* rounds run in latency mode           */
 } gd_server_stats_t;
 
 void gd_server_config_default(gd_server_config_t *cfg);
