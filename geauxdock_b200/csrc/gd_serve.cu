@@ -85,11 +85,15 @@ struct gd_server {
   int precision = GD_PREC_FP32;
   int grid = 0, Pmax = 0, Kst = 0, lig_slots = 0;
   size_t smem = 0;
-  // adaptive latency mode (replica_warps < 0): the latency-mode launch shape,
-  // and the replica-warps one wave of it holds
-  TileConfig tcl{8, 2, 8};
-  int grid_l = 0, Kst_l = 0;
-  long long wave_l = 0;
+  // adaptive latency mode (replica_warps = -G): the launch shapes of G, G/2, ...
+  // 2 warps per replica, largest first, each with the replicas one wave holds
+  struct Level {
+    TileConfig tc{8, 2, 8};
+    int grid = 0, Kst = 0;
+    long long wave = 0;
+  };
+  Level lv[3];
+  int nlv = 0;
   int max_items = 0;
   // device tables
   DevJob *d_jobs = nullptr;
@@ -249,11 +253,14 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
     any_fresh |= r->fresh;
     nrep_act += r->nrep;
   }
-  // adaptive latency mode: a round whose replicas, each on tcl.group warps,
-  // fit one wave of the grid runs in latency mode
-  const bool lat = s->tcl.group > 1 && nrep_act <= s->wave_l;
-  const TileConfig &tc = lat ? s->tcl : s->tc;
-  const int grid = lat ? s->grid_l : s->grid;
+  // adaptive latency mode: the most warps per replica whose one wave holds the
+  // round's replicas; one warp per replica when none does
+  int li = -1;
+  for (int i = 0; i < s->nlv && li < 0; ++i)
+    if (nrep_act <= s->lv[i].wave) li = i;
+  const bool lat = li >= 0;
+  const TileConfig &tc = lat ? s->lv[li].tc : s->tc;
+  const int grid = lat ? s->lv[li].grid : s->grid;
   // job table of this round
   DevJob *hj = s->h_jobs[b];
   for (int i = 0; i < nslot; ++i) hj[i] = DevJob{};
@@ -290,7 +297,7 @@ int enqueue_round(gd_server *s, long long k, std::vector<ServeReq *> &finishing,
   a.queue = s->d_queue;
   a.err = s->d_err;
   a.P = tc.stage ? s->Pmax : 0;
-  a.Kst = lat ? s->Kst_l : s->Kst;
+  a.Kst = lat ? s->lv[li].Kst : s->Kst;
   a.lig_slots = s->lig_slots;
   a.group = (uint16_t)tc.group;
   int launches = 0;
@@ -530,11 +537,12 @@ int server_configure(gd_server *s)
   // of uneven jobs) than two, with the same latency below saturation
   if (s->cfg.max_active_replicas <= 0)
     s->cfg.max_active_replicas = 4 * s->grid * (s->tc.warps_per_cta / s->tc.group);
-  if (s->tcl.group > 1) {
+  for (int i = 0; i < s->nlv; ++i) {
+    gd_server::Level &l = s->lv[i];
     size_t smem_l = 0;
     int occ_l = 0;
-    GD_TRY(choose_shape(s, s->tcl, s->grid_l, s->Kst_l, smem_l, occ_l));
-    s->wave_l = (long long)s->grid_l * (s->tcl.warps_per_cta / s->tcl.group);
+    GD_TRY(choose_shape(s, l.tc, l.grid, l.Kst, smem_l, occ_l));
+    l.wave = (long long)l.grid * (l.tc.warps_per_cta / l.tc.group);
   }
   return GD_OK;
 }
@@ -588,13 +596,17 @@ int server_create(const gd_pocket_desc_t *pockets, int npocket, const EnePara *e
     return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8; -2, -4 or -8: adaptive)", rw);
   if (adapt && adapt != 2 && adapt != 4 && adapt != 8)
     return fail(GD_E_INVALID, "replica_warps = %d (1, 2, 4 or 8; -2, -4 or -8: adaptive)", rw);
-  s->tcl = TileConfig{8, (int)o_kpl, (int)o_ab};
-  s->tcl.group = adapt;
   default_pair_tile(s->tc.group, s->tc.kpl, s->tc.ab);
-  default_pair_tile(std::max(adapt, 2), s->tcl.kpl, s->tcl.ab);
-  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1, s->tcl.group = 0;
+  if (s->precision == GD_PREC_FP64) s->tc.kpl = 1, s->tc.ab = 8, s->tc.group = 1;
   if (s->tc.kpl % 2) s->tc.group = 1;  // the split form exists for the FP32 atom-pair loop
-  if (s->tcl.kpl % 2) s->tcl.group = 0;
+  s->nlv = 0;
+  for (int g = adapt; g >= 2 && s->precision != GD_PREC_FP64; g /= 2) {
+    TileConfig t{8, (int)o_kpl, (int)o_ab};
+    t.group = g;
+    default_pair_tile(g, t.kpl, t.ab);
+    if (t.kpl % 2) break;  // the split form exists for the FP32 atom-pair loop
+    s->lv[s->nlv++].tc = t;
+  }
   GD_TRY(server_configure(s));
   s->max_items = s->cfg.max_active_replicas * 2 + s->cfg.max_replicas_per_job;
   GD_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));

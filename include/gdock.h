@@ -306,10 +306,11 @@ typedef struct gd_server_config {
   int device;
   int replica_warps;        /* warps per replica, 1 (default), 2, 4 or 8: latency mode, every
                                replica's pair rows and KDE points split over that many warps;
-                               -2, -4 or -8: adaptive, a round whose active replicas times that
-                               many warps fit the grid's resident warps runs in latency mode,
-                               others one warp per replica (a request's results then depend on
-                               the load it met, within the parity tolerance either way) */
+                               -2, -4 or -8: adaptive, each round on the most warps per replica
+                               (that many, or a power of two below it) for which one wave of
+                               the grid holds its active replicas, else one warp per replica (a
+                               request's results then depend on the load it met, within the
+                               parity tolerance either way) */
 } gd_server_config_t;
 
 typedef struct gd_request {

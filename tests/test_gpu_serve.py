@@ -207,11 +207,11 @@ def test_latency_mode_same_alone_and_in_mix(lib, enepara):
 
 
 def test_adaptive_latency_mode(lib, enepara):
-    """replica_warps = -4: a round whose replicas fit one wave on 4 warps each
-    runs in latency mode, others one warp per replica.  A small request gives
-    the bytes of the fixed latency-mode server; a request with more replicas
-    than one latency-mode wave holds (about a thousand on a B200) gives the
-    bytes of the one-warp server."""
+    """replica_warps = -4: a round runs on 4 warps per replica when one wave of
+    that split holds its replicas, else on 2 when one wave of that does, else on
+    one.  A small request gives the bytes of the fixed 4-warp server; a request
+    with more replicas than a 2-warp wave holds (about two thousand on a B200)
+    gives the bytes of the one-warp server."""
     pockets = _pockets()
     jobs = _jobs(pockets, 4, seed=9)
     small = (jobs[0], 100, 25)
@@ -221,10 +221,10 @@ def test_adaptive_latency_mode(lib, enepara):
     for f in fixed[0]["replicas"].dtype.names:
         assert fixed[0]["replicas"][f].tobytes() == adapt[0]["replicas"][f].tobytes(), f
     rng = np.random.default_rng(77)
-    big_job = synth.make_job(rng, pockets[1], 30, 32, 150, 5, synth.ladder(16, 0.3, 3.0), seed=501, pocket_index=1)
-    big = (big_job, 40, 20)                       # 32 x 3 x 16 = 1536 replicas
-    one, _ = _serve(pockets, enepara, [big], max_replicas_per_job=2048)
-    adapt2, st2 = _serve(pockets, enepara, [big], replica_warps=-4, max_replicas_per_job=2048)
+    big_job = synth.make_job(rng, pockets[1], 30, 48, 150, 5, synth.ladder(32, 0.3, 3.0), seed=501, pocket_index=1)
+    big = (big_job, 40, 20)                       # 48 x 3 x 32 = 4608 replicas
+    one, _ = _serve(pockets, enepara, [big], max_replicas_per_job=8192, max_jobs=4)
+    adapt2, st2 = _serve(pockets, enepara, [big], replica_warps=-4, max_replicas_per_job=8192, max_jobs=4)
     assert st2["completed"] == 1 and st2["latency_rounds"] == 0 < st2["rounds"]
     for f in one[0]["replicas"].dtype.names:
         assert one[0]["replicas"][f].tobytes() == adapt2[0]["replicas"][f].tobytes(), f
