@@ -183,6 +183,21 @@ def _config(n_rep: int, world: int, extra: dict | None = None) -> dict:
     return c
 
 
+def _cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the CPU baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+REF_BUILD = "g++ -O3 -fopenmp (the reference's Intel #pragma simd hints are ignored by g++)"
+
+
 def cpu_reference_sample(cx, seconds: float) -> dict:
     """The reference's own CPU Monte Carlo (MonteCarlo_d, OpenMP over replicas) on
     all replicas of the complex for a number of steps sized to ~`seconds`."""
@@ -208,6 +223,7 @@ def cpu_reference_sample(cx, seconds: float) -> dict:
     ref.gdref_montecarlo(work.ctypes.data, rec.ctypes.data, 2, steps)
     dt = time.perf_counter() - t0
     return {"value": n * steps / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "cpu_model": _cpu_model(), "build": REF_BUILD,
             "sample": f"{n} replicas x {steps} MC steps of the same complex, reference MonteCarlo_d "
                       f"(g++ -O3 -fopenmp, OMP_NUM_THREADS={cores}), {dt:.1f} s"}
 
@@ -255,7 +271,8 @@ def run_reference(args) -> None:
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, Astex-like shapes)",
         "config": _config(n, world), "impl": "reference", "sample": sample,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                         "cpu_model": _cpu_model(), "build": REF_BUILD},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "libraries_loaded": O.mapped_libraries(ROOT)}))
 
