@@ -61,6 +61,9 @@ STEPS_PER_INTERVAL = 50
 #       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,4,8,0
 # (1,851,392 B read + 59,392 B written); it does not grow with the steps per launch.
 TRAFFIC_BYTES_PER_LAUNCH = 1_851_392 + 59_392
+# L2 sectors of the small-case ncu --set full capture of the same kernel (3520 replicas x 4 steps,
+# profiles/mc_kernel_ensemble3520_small_full.md): 32 B each, per pose-eval
+L2_BYTES_PER_POSE_EVAL = 14_664_739 * 32 / (3520 * 4)
 TRAFFIC_SOURCE = ("recorded constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                   "kernel of commit 57b8d54, profiles/mc_kernel_ensemble3520_traffic.md")
 
@@ -287,6 +290,15 @@ def _hbm_share(launch_ms: float) -> dict:
     gbs = TRAFFIC_BYTES_PER_LAUNCH / (launch_ms / 1e3) / 1e9
     return {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak if peak else None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peak else "unavailable"}
+
+
+def _l2_rate(pose_evals_per_s: float) -> dict:
+    """L2 bandwidth the batched kernel moves at this run's rate, from the recorded
+    per-pose-eval L2 sectors of its small-case capture (no measured L2 peak exists
+    to divide by)."""
+    return {"achieved_gbs": L2_BYTES_PER_POSE_EVAL * pose_evals_per_s / 1e9,
+            "source": "recorded constant: lts__t_sectors.sum x 32 B of the small-case capture per pose-eval "
+                      "(profiles/mc_kernel_ensemble3520_small_full.md) x this run's pose-evals/s"}
 
 
 def _mufu_share(natom: int, npoint: int, pose_evals_per_s: float, sm_mhz) -> dict:
@@ -789,6 +801,7 @@ def run_ours(args) -> None:
                          "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                          "traffic_source": TRAFFIC_SOURCE,
                          "hbm": _hbm_share(avg_launch_ms) if spi == STEPS_PER_INTERVAL else None,
+                         "l2": _l2_rate(n_rep * spi / (avg_launch_ms / 1e3)),
                          "kernel": "gd::mc_kernel (batched Monte Carlo, 50 steps x 3520 replicas per launch)",
                          "flops_per_pose_eval": fpp, "avg_launch_ms": avg_launch_ms,
                          "peak_source": "measured this run: FP32 FMA microbenchmark gd_fp32_peak (2 flops/FMA); "
