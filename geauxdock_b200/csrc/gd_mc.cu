@@ -724,23 +724,59 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
           }
         }
       }
+      if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+        // the block's AB contact sums reduced across the warp together: each
+        // butterfly step halves the sums a lane carries (it keeps the half its
+        // lane bit selects and adds its partner's copy of it), then plain steps
+        // finish; lane l ends with atom a0 + base's sum, as do the lanes that
+        // differ from it below bit log2(32 / AB).  One lane per atom applies the
+        // restraint; its per-lane terms are summed once after the last block.
+        float v[AB];
 #pragma unroll
-      for (int k = 0; k < AB; ++k) {
-        const int a = a0 + k;
-        if (a >= L) break;
-        const T S = warp_sum(hpc[k]);
-        if constexpr (SPLIT && PREC != kFP64) {
-          if (G > 1) {
-            // this warp's share of atom a's contact sum; the restraint comes after the combination
-            if (lane == 0) sp.gparts[sp.sub * sp.pstride + kPartTerms + a] = (float)S;
-            continue;
+        for (int k = 0; k < AB; ++k) v[k] = hpc[k];
+        int base = 0;
+#pragma unroll
+        for (int n = AB, off = 16; n > 1; n >>= 1, off >>= 1) {
+          const bool hi = (lane & off) != 0;
+#pragma unroll
+          for (int i = 0; i < n / 2; ++i) {
+            const float keep = hi ? v[n / 2 + i] : v[i], give = hi ? v[i] : v[n / 2 + i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, give, off);
+          }
+          base += hi ? n / 2 : 0;
+        }
+#pragma unroll
+        for (int off = 16 / AB; off > 0; off >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], off);
+        const int a = a0 + base;
+        if (a < L && (lane & (32 / AB - 1)) == 0) {
+          bool restraint = true;
+          if constexpr (SPLIT) {
+            if (G > 1) {
+              // this warp's share of atom a's contact sum; the restraint comes after the combination
+              sp.gparts[sp.sub * sp.pstride + kPartTerms + a] = v[0];
+              restraint = false;
+            }
+          }
+          if (restraint) {
+            const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
+            const float h2 = (v[0] - par->hpl0[lt]) / par->hpl1[lt];
+            ehpc += 0.5f * h2 * h2 - par->hpl2[lt];
           }
         }
-        const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
-        const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
-        ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
+      } else {
+#pragma unroll
+        for (int k = 0; k < AB; ++k) {
+          const int a = a0 + k;
+          if (a >= L) break;
+          const T S = warp_sum(hpc[k]);
+          const int lt = GD_AT(lgrp[GD_AT(a, L, kSiteLgrp)].x, kLigTypes, kSiteTab);
+          const T h2 = (S - (T)par->hpl0[lt]) / (T)par->hpl1[lt];
+          ehpc += (T)0.5 * h2 * h2 - (T)par->hpl2[lt];
+        }
       }
     }
+    // the atom-pair form's restraint terms sit on one lane per atom
+    if constexpr (PREC != kFP64 && KPL % 2 == 0) ehpc = warp_sum(ehpc);
   }
 
   T vdw, ele, pmf, psp, hdb;
