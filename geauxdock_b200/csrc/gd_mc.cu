@@ -99,7 +99,9 @@ __device__ __forceinline__ long long check_at(long long i, long long n, int site
 #else
 // unparenthesised on purpose: the index expression keeps its own grouping
 // (a pointer plus an index sum is then computed as written), so that the
-// product build compiles to exactly the code without the checks
+// product build compiles to exactly the code without the checks.  A use
+// inside a product or another operator must parenthesise its argument
+// (2 * GD_AT((k + m), ...)), or it would expand to 2 * k + m.
 #define GD_AT(i, n, site) i
 #define GD_CHECK_ARG(...)
 #endif
