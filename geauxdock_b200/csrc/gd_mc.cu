@@ -655,13 +655,18 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
         // sums of atoms a0 + 2k and a0 + 2k + 1 (AB is even) of hpp (y^2 (y + y^2)),
         // twice the contact sum (halved exactly at the end)
         const float2 one = f2(1.0f), c1 = f2(-1.0f / 81.0f);
+        // rows of at most 64 points here: the last row of the hydrophobic-contact
+        // points then carries at most 63 others (hpp 0) where 128-point rows
+        // would carry up to 127
+        constexpr int K2 = KPL > 2 ? 2 : KPL;
+        const int rows2 = ((J.ncdc[iprt] + 32 * K2 - 1) / (32 * K2)) * (32 * K2);
         float2 h2[AB / 2];
 #pragma unroll
         for (int k = 0; k < AB / 2; ++k) h2[k] = f2(0.0f);
-        for (int row = row0; row < rows; row += rstep) {
-          float2 npx[KPL], npy[KPL], npz[KPL], ph2[KPL];
+        for (int row = 32 * K2 * my_sub; row < rows2; row += 32 * K2 * G) {
+          float2 npx[K2], npy[K2], npz[K2], ph2[K2];
 #pragma unroll
-          for (int j = 0; j < KPL; ++j) {
+          for (int j = 0; j < K2; ++j) {
             const int p = GD_AT(row + 32 * j + lane, P, kSitePos);
             const float4 q = pos[p];
             npx[j] = f2(-q.x);
@@ -675,7 +680,7 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
             if (a >= L) break;
             const LigPair la = lig[GD_AT(a >> 1, (L + 1) >> 1, kSiteLig)];
 #pragma unroll
-            for (int j = 0; j < KPL; ++j) {
+            for (int j = 0; j < K2; ++j) {
               const float2 dx = __fadd2_rn(la.x, npx[j]), dy = __fadd2_rn(la.y, npy[j]), dz = __fadd2_rn(la.z, npz[j]);
               const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
               float2 y = __ffma2_rn(d2, c1, one);
