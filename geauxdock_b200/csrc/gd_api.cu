@@ -567,6 +567,7 @@ int dock_refill_device(gd_ensemble *e, const Complex *d_cx, int rb, int re, int 
   D.pcell = const_cast<int4 *>(J.pcell);
   D.pcell_cnt = const_cast<int *>(J.pcell_cnt);
   D.pcell_stride = J.pcell_stride;
+  D.kslot = const_cast<int4 *>(J.kslot);
   D.kde_cap = std::max(J.nkde, 1);
   D.Ppad = pk.Ppad;
   D.nkde_expect = J.nkde;

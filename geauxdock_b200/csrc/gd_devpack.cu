@@ -244,6 +244,46 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
   }
   if (tid == 0 && s_nk == 0 && D.kde_cap > 0) D.kde[0] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
+  // KDE slots (the host packer's order): for each ligand type group, each KDE
+  // point of its type, with the group's atom range and 1/(points of the type)
+  __shared__ int s_ga[kLigTypes], s_ge[kLigTypes], s_gt[kLigTypes], s_go[kLigTypes + 1], s_ng, s_valid;
+  // (only for a valid Complex: with an out-of-range ligand type the grouped
+  // order does not cover every atom)
+  if (tid == 0) s_valid = (*(volatile int *)D.err & kErrPack) == 0;
+  __syncthreads();
+  if (D.kslot && s_valid) {
+    if (tid == 0) {
+      int ng = 0, off = 0;
+      for (int a = 0; a < L;) {
+        const int t = s_ltype[a];
+        int e = a;
+        while (e < L && s_ltype[e] == t) ++e;
+        if (s_kcnt[t] > 0) {
+          s_ga[ng] = a;
+          s_ge[ng] = e;
+          s_gt[ng] = t;
+          s_go[ng] = off;
+          off += s_kcnt[t];
+          ++ng;
+        }
+        a = e;
+      }
+      s_go[ng] = off;
+      s_ng = ng;
+    }
+    __syncthreads();
+    const int nslot = s_go[s_ng];
+    for (int q = tid; q < nslot && q < D.kde_cap; q += blockDim.x) {
+      int g = 0;
+      while (q >= s_go[g + 1]) ++g;
+      const int t = s_gt[g];
+      const float4 p = D.kde[s_kbeg[t] + (q - s_go[g])];
+      const float inv = 1.0f / (float)s_kcnt[t];
+      D.kslot[2 * q] = make_int4(__float_as_int(p.x), __float_as_int(p.y), __float_as_int(p.z), __float_as_int(inv));
+      D.kslot[2 * q + 1] = make_int4(s_ga[g] | (s_ge[g] << 16), 0, 0, 0);
+    }
+    __syncthreads();
+  }
   // the header only for a valid Complex: the kernels that read it run only then
   if (tid == 0 && (*(volatile int *)D.err & kErrPack) == 0) {
     DevJob J;
@@ -270,6 +310,8 @@ __global__ void dp_setup_kernel(const Complex *__restrict__ cx, PackDst D)
     }
     J.nkde = s_nk;
     J.kde = D.kde;
+    J.nkslot = (D.kslot && s_valid) ? min(s_go[s_ng], D.kde_cap) : 0;
+    J.kslot = D.kslot;
     J.nmcs = M;
     J.mcs = D.mcs;
     J.tcc = D.tcc;

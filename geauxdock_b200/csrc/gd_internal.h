@@ -134,6 +134,12 @@ struct DevJob {
   const float4 *kde;       // [nkde]
   int kbeg[kLigTypes];
   int kcnt[kLigTypes];
+  // the same as a list of (KDE point, ligand type group) slots, one per KDE point of a type the
+  // ligand has, in the grouped ligand's type order: slot s is the int4 pair kslot[2 s + {0, 1}] =
+  // (bits of x, y, z of the point and of 1/(points of its type)), (beg | end << 16, 0, 0, 0),
+  // [beg, end) the group's atoms; nkslot <= nkde (the atom-pair form's KDE pass)
+  int nkslot;
+  const int4 *kslot;
   // MCS
   int nmcs;
   const float4 *mcs;       // [L][nmcs]

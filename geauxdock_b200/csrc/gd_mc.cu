@@ -805,11 +805,33 @@ __device__ __noinline__ void energy_warp(const DevJob &J, const DevParams *__res
 
   // ---- KDE, energy_kde_v1.cu:183-274: per atom, mean of exp(kde2 d^2) over
   // the KDE points of the same type; atoms with no such point contribute 0.
-  // One type group at a time: lane k holds KDE point k of the group's type and
+  // The atom-pair form walks the job's slots (below); the per-type-group form:
+  // one type group at a time, lane k holds KDE point k of the group's type and
   // sums over the group's atoms, then scales by 1 / (points of the type).  A
-  // replica split over G warps deals the type groups out to its warps in turn.
+  // replica split over G warps deals the slots or the type groups out to its
+  // warps in turn.
   T kacc = 0;
-  {
+  if constexpr (PREC != kFP64 && KPL % 2 == 0) {
+    // the atom-pair form walks the job's KDE slots: lane k takes slot k (one
+    // KDE point of one of the ligand's type groups) and sums over the group's
+    // atoms, weighted by 1/(points of the type): every lane busy, one
+    // coalesced pair of loads per slot, no division
+    const float k2 = par->kde2 * kLog2e;
+    for (int q = 32 * my_sub + lane; q < J.nkslot; q += 32 * G) {
+      const int4 c0 = __ldg(J.kslot + 2 * GD_AT(q, J.nkde, kSiteKde));
+      const int4 c1 = __ldg(J.kslot + 2 * q + 1);
+      const float qx = __int_as_float(c0.x), qy = __int_as_float(c0.y), qz = __int_as_float(c0.z);
+      float sk = 0.0f;
+      const int end = c1.x >> 16;
+      for (int b = c1.x & 0xffff; b < end; ++b) {
+        const V4<float> la = atom_at(lig, GD_AT(b, L, kSiteLig));
+        const float dx = la.x - qx, dy = la.y - qy, dz = la.z - qz;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        sk += ex2_approx(k2 * d2);
+      }
+      kacc += sk * __int_as_float(c0.w);
+    }
+  } else {
     const T kde2 = par->kde2;
     int tg = 0;
     for (int a = 0; a < L; ++tg) {

@@ -508,6 +508,22 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
     if (kcnt[t] == 0) kbeg[t] = (int)j;
     ++kcnt[t];
   }
+  // KDE slots: for each ligand type group (grouped order), each KDE point of its type
+  std::vector<int4> kslot;
+  for (int a = 0; a < L;) {
+    const int t = ltype[a], e = lgend[a];
+    if (kcnt[t] > 0) {
+      const float inv = 1.0f / (float)kcnt[t];
+      for (int k = kbeg[t]; k < kbeg[t] + kcnt[t]; ++k) {
+        kslot.push_back(make_int4(as_int(kde[k].x), as_int(kde[k].y), as_int(kde[k].z), as_int(inv)));
+        kslot.push_back(make_int4(a | (e << 16), 0, 0, 0));
+      }
+    }
+    a = e;
+  }
+  const int nkslot = (int)(kslot.size() / 2);
+  // room for any ligand of the same shapes (a refill on the GPU): one slot per KDE point
+  kslot.resize(2 * (size_t)std::max<size_t>(kidx.size(), 1), make_int4(0, 0, 0, 0));
 
   // MCS templates, atom-major in grouped order; validity as energy_mcs_v1.cu:295
   std::vector<float4> mcs((size_t)L * jd.M);
@@ -610,7 +626,7 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   Arena ar;
   const size_t o_par = ar.put(parv), o_lig = ar.put(lig), o_lg = ar.put(lgrp), o_lc = ar.put(jd.lcenter);
   const size_t o_pm = ar.put(pspmask), o_hr = ar.put(ref4);
-  const size_t o_pc = ar.put(pcell), o_pcn = ar.put(pcell_cnt);
+  const size_t o_pc = ar.put(pcell), o_pcn = ar.put(pcell_cnt), o_ks = ar.put(kslot);
   const size_t o_kde = ar.put(kde), o_mcs = ar.put(mcs), o_tcc = ar.put(jd.tcc), o_psp = ar.put(psp);
   const size_t o_mb = ar.put(jd.minus_beta), o_rep = ar.put(jd.reps), o_acc = ar.put(run_acc), o_st = ar.put(stats);
   size_t o_rec = 0;
@@ -662,6 +678,8 @@ int pack_job_impl(const JobData &jd, const DevPocket &pk, const EnePara &ep, boo
   J.pcell_cnt = (const int *)(b + o_pcn);
   J.pcell_stride = cstride;
   J.nkde = (int)kidx.size();
+  J.nkslot = nkslot;
+  J.kslot = (const int4 *)(b + o_ks);
   J.kde = (const float4 *)(b + o_kde);
   for (int t = 0; t < kLigTypes; ++t) {
     J.kbeg[t] = kbeg[t];

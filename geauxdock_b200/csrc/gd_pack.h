@@ -152,6 +152,7 @@ struct PackDst {
   float *psp;
   uint32_t *pspmask;
   int4 *pcell;         // pocket-specific cells (nullptr: none; only the per-type-group form reads the job)
+  int4 *kslot;         // KDE slots, kde_cap of them (nullptr: none, as pcell)
   int *pcell_cnt;
   int pcell_stride;    // cells per conformation the array holds
   int kde_cap;         // KDE points the kde array holds
