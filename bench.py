@@ -55,17 +55,17 @@ STEPS_PER_INTERVAL = 50
 # DRAM bytes (read + write) of one Monte Carlo launch of this workload (3520
 # replicas x 50 steps, tile 8 x kpl 4 x ab 8, pocket read through L1): a RECORDED
 # constant, not measured by this script.  From one capture on a B200 of the kernel
-# of commit e8e2f21 (profiles/mc_kernel_ensemble3520_traffic.md):
+# of commit ecc5177 (profiles/mc_kernel_ensemble3520_traffic.md):
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:mc_kernel -s 4 -c 1
 #       python bench.py --steps 3 --warmup 3 --workload ensemble --skip-extras --tile 8,4,8,0
-# (1,545,472 B read + 121,856 B written); it does not grow with the steps per launch.
-TRAFFIC_BYTES_PER_LAUNCH = 1_545_472 + 121_856
+# (1,742,848 B read + 75,008 B written); it does not grow with the steps per launch.
+TRAFFIC_BYTES_PER_LAUNCH = 1_742_848 + 75_008
 # L2 sectors of the small-case ncu --set full capture of the same kernel (3520 replicas x 4 steps,
 # profiles/mc_kernel_ensemble3520_small_full.md): 32 B each, per pose-eval
-L2_BYTES_PER_POSE_EVAL = 15_167_009 * 32 / (3520 * 4)
+L2_BYTES_PER_POSE_EVAL = 14_684_063 * 32 / (3520 * 4)
 TRAFFIC_SOURCE = ("recorded constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
-                  "kernel of commit e8e2f21, profiles/mc_kernel_ensemble3520_traffic.md")
+                  "kernel of commit ecc5177, profiles/mc_kernel_ensemble3520_traffic.md")
 
 
 def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
