@@ -20,9 +20,11 @@
 // instruction (sm_100).  Per work item the CTA builds from the per-type tables
 // one entry per (atom pair, point type) with the two atoms' values interleaved,
 // so the loop walks atom pairs with no grouping by atom type; the sparse
-// hydrogen-bond and pocket-specific terms are evaluated only for the atom pairs
-// where some point of the row needs them.  With KPL = 1 (and in FP64) the atoms
-// are walked one type group at a time in scalar arithmetic instead.  Pass 2
+// hydrogen-bond term is evaluated only for the atom pairs where some point of
+// the row needs it, and the pocket-specific term is walked after the loop over
+// the potential's non-zero cells of the conformation.  With KPL = 1 (and in
+// FP64) the atoms are walked one type group at a time in scalar arithmetic,
+// the pocket-specific term inside that loop.  Pass 2
 // (the hydrophobic contact) visits only the rows holding cdc == 1 points, packed
 // over atom pairs the same way, and keeps per-atom sums in registers for AB
 // atoms at a time.
