@@ -21,8 +21,8 @@ among the poses where |e64_i| < TAU[i], measured over the 10^6 poses of the
 precision workload (64 atoms x 3000 points x 1000 KDE points, the largest sums
 of the test workloads; tests/test_gpu_precision.py reports it): the
 electrostatic and hydrophobic sums cancel most (charges of both signs;
-per-atom quadratics minus hpl2; 1.3e-6 and 1.5e-6 there), the KDE and MCS
-sums least (below 1.4e-7).  Terms that never fell below 0.25 on that workload
+per-atom quadratics minus hpl2; at most 1.4e-6 and 1.5e-6 there over the
+kernels measured), the KDE and MCS sums least (below 1.4e-7).  Terms that never fell below 0.25 on that workload
 (Lennard-Jones, pmf, hydrogen bond, distance, total) keep 0.25.
 
 The pocket-specific term (index 3) is in addition a step function of the
